@@ -1,0 +1,1605 @@
+// Batched SQP + Schur-complement PCG solver and its adjoint for sm_100a.
+//
+// One CTA solves one instance from start to finish: the SQP loop of
+// diffmpc/solvers/sqp.py:436-560 (linearize -> assemble S, Phi^-1, gamma ->
+// PCG -> recover (x, u) -> optional line search -> convergence test) runs
+// entirely on the device with per-instance early exit, and the adjoint
+// (sqp.py:668-798) reuses the same building blocks.  The grid holds every
+// instance of every group, so one launch solves a ragged, mixed-model batch and
+// the hardware block scheduler balances uneven instances across the 148 SMs.
+//
+// Precision.  DMPC_PREC_FP64 runs the reference's FP64 PCG recurrence.
+// DMPC_PREC_MIXED keeps the block rows of S and Phi^-1 in FP32 in shared
+// memory, runs the PCG iterations in FP32 (dot products accumulated in FP64)
+// and wraps them in FP64 iterative refinement: the residual gamma - S lambda
+// and the stopping test eta = r^T Phi^-1 r <= eps use the FP64 blocks, so the
+// reference's absolute stopping rule (pcg.py:397-403) is applied in FP64.
+//
+// Storage of the Schur system (compact, symmetric block-tridiagonal):
+//   S row t      = -[phi_{t-1}, theta_t, phi_t^T]          (pcg.py:198-211)
+//   Phi^-1 row t =  [P_t, theta_t^-1, P_{t+1}^T],  P_t = -theta_t^-1 phi_{t-1} theta_{t-1}^-1
+//                                                           (pcg.py:213-239)
+// so each operator is one diagonal block per knot and one off-diagonal block per
+// stage; the reference's third column block of Phi^-1 equals P_{t+1}^T because
+// the theta blocks are symmetric.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "../../include/dmpc.h"
+#include "common.cuh"
+#include "dual.cuh"
+#include "models.cuh"
+
+namespace {
+
+constexpr int kMaxGroups = 8;
+
+struct DevGroup {
+  dmpc_group g;
+  dmpc_adjoint a;
+  int32_t first_block;  // first grid block of this group
+  int32_t K;            // horizon + 1
+  int32_t ld32;         // row stride of FP32 blocks (odd, >= nx)
+  int32_t blocks_smem;  // FP32 blocks live in shared memory
+  size_t ws_offset;     // byte offset of instance 0 in the workspace
+  size_t ws_stride;     // bytes per instance
+  int32_t pg_idx[DMPC_MAX_PARAM_GRADS];
+};
+
+struct DevArgs {
+  int32_t n_groups;
+  int32_t total_blocks;
+  dmpc_solver_params p;
+  DevGroup grp[kMaxGroups];
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// ---------------------------------------------------------------- workspace layout
+struct Layout {
+  // offsets in doubles
+  size_t A, Bm, C, Qi, Ri, q, r, gam, lam, res, t1, xb, ub, xn, un, fv, th, ph, ti, pm, tmp, contrib;
+  size_t n_doubles;
+  size_t f32;  // float offset (in floats) after the doubles, FP32 blocks when not in smem
+  size_t n_floats;
+  size_t bytes;
+};
+
+__host__ __device__ inline Layout make_layout(int nx, int nu, int N, int ld32, bool blocks_global,
+                                              int n_param_grads) {
+  Layout L;
+  const size_t K = N + 1;
+  size_t o = 0;
+  auto take = [&](size_t n) {
+    size_t r = o;
+    o += align_up(n, 4);
+    return r;
+  };
+  L.A = take((size_t)N * nx * nx);
+  L.Bm = take((size_t)N * nx * nu);
+  L.C = take(K * nx);
+  L.Qi = take(K * nx);
+  L.Ri = take(K * nu);
+  L.q = take(K * nx);
+  L.r = take(K * nu);
+  L.gam = take(K * nx);
+  L.lam = take(K * nx);
+  L.res = take(K * nx);
+  L.t1 = take(K * nx);
+  L.xb = take(K * nx);
+  L.ub = take(K * nu);
+  L.xn = take(K * nx);
+  L.un = take(K * nu);
+  L.fv = take(K * nx);
+  L.th = take(K * nx * nx);
+  L.ph = take((size_t)N * nx * nx + nx * nx);
+  L.ti = take(K * nx * nx);
+  L.pm = take((size_t)N * nx * nx + nx * nx);
+  L.tmp = take(K * nx * nx);
+  L.contrib = take((size_t)(n_param_grads > 0 ? (n_param_grads < DMPC_MAX_PARAM_GRADS ? n_param_grads : DMPC_MAX_PARAM_GRADS) : 1) * K);
+  L.n_doubles = o;
+  L.f32 = 0;
+  L.n_floats = blocks_global ? align_up((size_t)4 * K * nx * ld32, 8) : 0;
+  L.bytes = align_up(L.n_doubles * 8 + L.n_floats * 4, 256);
+  return L;
+}
+
+__host__ __device__ inline int odd_ld(int nx) { return (nx % 2 == 0) ? nx + 1 : nx; }
+
+// shared memory bytes of one CTA: 2x32 reduction doubles + PCG vectors (+ FP32 blocks)
+__host__ __device__ inline size_t smem_bytes_for(int nx, int N, int precision, bool blocks_smem) {
+  const size_t K = N + 1;
+  size_t b = 64 * sizeof(double) + 64;  // reductions + flags
+  if (precision == DMPC_PREC_FP64) {
+    b += 5 * K * nx * sizeof(double);
+  } else {
+    b += align_up(5 * K * nx * sizeof(float), 16);
+    if (blocks_smem) b += (size_t)4 * K * nx * odd_ld(nx) * sizeof(float);
+  }
+  return align_up(b, 16);
+}
+
+// ---------------------------------------------------------------- instance context
+struct Inst {
+  int model, nx, nu, N, K, scheme, pen, P, ld;
+  double dt;
+  const double *x0, *xf, *xref, *uref, *wx, *wu, *wf, *mp;
+  double *A, *Bm, *C, *Qi, *Ri, *q, *r, *gam, *lam, *res, *t1, *xb, *ub, *xn, *un, *fv;
+  double *th, *ph, *ti, *pm, *tmp, *contrib;
+  float *th32, *ph32, *ti32, *pm32;
+};
+
+__device__ inline Inst make_inst(const DevGroup& G, int i, void* ws, float* smem_blocks) {
+  const dmpc_group& g = G.g;
+  Inst s;
+  s.model = g.model;
+  s.nx = g.nx;
+  s.nu = g.nu;
+  s.N = g.horizons ? g.horizons[i] : g.horizon;
+  s.K = s.N + 1;
+  s.scheme = g.scheme;
+  s.pen = g.penalize_control_reference;
+  s.P = g.n_model_params;
+  s.ld = G.ld32;
+  s.dt = g.dt[i];
+  const int nx = g.nx, nu = g.nu, Kmax = G.K;
+  s.x0 = g.initial_state + (size_t)i * nx;
+  s.xf = g.final_state + (size_t)i * nx;
+  s.xref = g.reference_state + (size_t)i * Kmax * nx;
+  s.uref = g.reference_control + (size_t)i * Kmax * nu;
+  s.wx = g.w_x + (size_t)i * nx;
+  s.wu = g.w_u + (size_t)i * nu;
+  s.wf = g.w_f + (size_t)i * nx;
+  s.mp = g.model_params + (size_t)i * g.n_model_params;
+  Layout L = make_layout(nx, nu, g.horizon, G.ld32, !G.blocks_smem, g.n_model_params);
+  double* base = reinterpret_cast<double*>(reinterpret_cast<char*>(ws) + G.ws_offset + (size_t)i * G.ws_stride);
+  s.A = base + L.A;
+  s.Bm = base + L.Bm;
+  s.C = base + L.C;
+  s.Qi = base + L.Qi;
+  s.Ri = base + L.Ri;
+  s.q = base + L.q;
+  s.r = base + L.r;
+  s.gam = base + L.gam;
+  s.lam = base + L.lam;
+  s.res = base + L.res;
+  s.t1 = base + L.t1;
+  s.xb = base + L.xb;
+  s.ub = base + L.ub;
+  s.xn = base + L.xn;
+  s.un = base + L.un;
+  s.fv = base + L.fv;
+  s.th = base + L.th;
+  s.ph = base + L.ph;
+  s.ti = base + L.ti;
+  s.pm = base + L.pm;
+  s.tmp = base + L.tmp;
+  s.contrib = base + L.contrib;
+  float* fb = G.blocks_smem ? smem_blocks : reinterpret_cast<float*>(base + L.n_doubles);
+  const size_t dblk = (size_t)s.K * nx * s.ld;  // diagonal blocks of this instance
+  const size_t oblk = (size_t)(s.N + 1) * nx * s.ld;
+  s.th32 = fb;
+  s.ti32 = fb + dblk;
+  s.ph32 = fb + 2 * dblk;
+  s.pm32 = fb + 2 * dblk + oblk;
+  return s;
+}
+
+// Linear model: integrator with the parameter matrices read from global memory.
+// Parameter `pk` (or -1) carries the hyper-dual e2 direction.
+template <class T>
+__device__ __forceinline__ T pcoef(double v, bool hit) {
+  return T(v);
+}
+template <>
+__device__ __forceinline__ HDual pcoef<HDual>(double v, bool hit) {
+  return HDual(v, 0.0, hit ? 1.0 : 0.0, 0.0);
+}
+
+template <class T>
+__device__ void linear_state_dot_mem(const Inst& s, const T* x, const T* u, T* xd, int pk) {
+  const int nx = s.nx, nu = s.nu;
+  const double* A = s.mp;
+  const double* B = A + nx * nx;
+  const double* b = B + nx * nu;
+  for (int i = 0; i < nx; ++i) {
+    T a = 0.0;
+    for (int j = 0; j < nx; ++j) a = a + pcoef<T>(A[i * nx + j], pk == i * nx + j) * x[j];
+    T c = 0.0;
+    for (int j = 0; j < nu; ++j) c = c + pcoef<T>(B[i * nu + j], pk == nx * nx + i * nu + j) * u[j];
+    xd[i] = a + c + pcoef<T>(b[i], pk == nx * nx + nx * nu + i);
+  }
+}
+
+template <class T>
+__device__ void predict_next_state_linear(const Inst& s, const T* x, const T* u, T* xn, int pk = -1) {
+  constexpr int MX = DMPC_MAX_NX;
+  const int nx = s.nx;
+  const double dt = s.dt;
+  T k[MX], tmp[MX], acc[MX];
+  linear_state_dot_mem(s, x, u, k, pk);
+  for (int i = 0; i < nx; ++i) xn[i] = x[i] + dt * k[i];
+  if (s.scheme == DMPC_MIDPOINT) {
+    for (int i = 0; i < nx; ++i) tmp[i] = x[i] + 0.5 * dt * k[i];
+    linear_state_dot_mem(s, tmp, u, acc, pk);
+    for (int i = 0; i < nx; ++i) xn[i] = x[i] + dt * acc[i];
+  } else if (s.scheme == DMPC_RK4) {
+    for (int i = 0; i < nx; ++i) {
+      acc[i] = k[i];
+      tmp[i] = x[i] + 0.5 * dt * k[i];
+    }
+    linear_state_dot_mem(s, tmp, u, k, pk);
+    for (int i = 0; i < nx; ++i) {
+      acc[i] = acc[i] + 2.0 * k[i];
+      tmp[i] = x[i] + 0.5 * dt * k[i];
+    }
+    linear_state_dot_mem(s, tmp, u, k, pk);
+    for (int i = 0; i < nx; ++i) {
+      acc[i] = acc[i] + 2.0 * k[i];
+      tmp[i] = x[i] + dt * k[i];
+    }
+    linear_state_dot_mem(s, tmp, u, k, pk);
+    for (int i = 0; i < nx; ++i) xn[i] = x[i] + ((1.0 / 6.0) * (acc[i] + k[i])) * dt;
+  }
+}
+
+// ---------------------------------------------------------------- linearization
+// One work item = (stage t, direction d): a Dual evaluation of the integrator
+// gives column d of [A_t | B_t] (value_and_jacfwd, jax_utils.py:12-36).
+template <int MODEL>
+__device__ void linearize_item(const Inst& s, const double* xb, const double* ub, int t, int d) {
+  constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
+  const int nx = s.nx, nu = s.nu;
+  Dual x[MX], u[MU], xn[MX];
+  for (int j = 0; j < nx; ++j) x[j] = Dual(xb[t * nx + j], j == d ? 1.0 : 0.0);
+  for (int j = 0; j < nu; ++j) u[j] = Dual(ub[t * nu + j], nx + j == d ? 1.0 : 0.0);
+  if (MODEL == DMPC_MODEL_LINEAR) {
+    // parameters as constants: read straight from memory to keep registers low
+    predict_next_state_linear(s, x, u, xn);
+  } else {
+    Dual p[12];
+    for (int k = 0; k < s.P && k < 12; ++k) p[k] = Dual(s.mp[k]);
+    predict_next_state<Dual, MODEL>(s.scheme, s.dt, nx, nu, x, u, p, xn);
+  }
+  if (d < nx) {
+    for (int i = 0; i < nx; ++i) s.A[((size_t)t * nx + i) * nx + d] = xn[i].d;
+  } else {
+    for (int i = 0; i < nx; ++i) s.Bm[((size_t)t * nx + i) * nu + (d - nx)] = xn[i].d;
+  }
+  if (d == 0)
+    for (int i = 0; i < nx; ++i) s.fv[t * nx + i] = xn[i].v;
+}
+
+// Plain FP64 integrator step for one stage (line search, constraint values).
+__device__ void next_state_value(const Inst& s, const double* x, const double* u, double* xn) {
+  switch (s.model) {
+    case DMPC_MODEL_LINEAR: predict_next_state_linear<double>(s, x, u, xn); break;
+    case DMPC_MODEL_QUADROTOR: predict_next_state<double, DMPC_MODEL_QUADROTOR>(s.scheme, s.dt, s.nx, s.nu, x, u, s.mp, xn); break;
+    case DMPC_MODEL_SPACECRAFT: predict_next_state<double, DMPC_MODEL_SPACECRAFT>(s.scheme, s.dt, s.nx, s.nu, x, u, s.mp, xn); break;
+    case DMPC_MODEL_ATTITUDE: predict_next_state<double, DMPC_MODEL_ATTITUDE>(s.scheme, s.dt, s.nx, s.nu, x, u, s.mp, xn); break;
+    case DMPC_MODEL_CARTPOLE: predict_next_state<double, DMPC_MODEL_CARTPOLE>(s.scheme, s.dt, s.nx, s.nu, x, u, s.mp, xn); break;
+  }
+}
+
+// A_t, B_t, f(x_t, u_t) for t < N, then C = [x0; -f + A x + B u]
+// (optimal_control_problem.py:325-398).  As_next = -I is implicit.
+__device__ void linearize_dynamics(const Inst& s, const double* xb, const double* ub) {
+  const int nd = s.nx + s.nu;
+  const int items = s.N * nd;
+  for (int w = threadIdx.x; w < items; w += blockDim.x) {
+    const int t = w / nd, d = w - t * nd;
+    switch (s.model) {
+      case DMPC_MODEL_LINEAR: linearize_item<DMPC_MODEL_LINEAR>(s, xb, ub, t, d); break;
+      case DMPC_MODEL_QUADROTOR: linearize_item<DMPC_MODEL_QUADROTOR>(s, xb, ub, t, d); break;
+      case DMPC_MODEL_SPACECRAFT: linearize_item<DMPC_MODEL_SPACECRAFT>(s, xb, ub, t, d); break;
+      case DMPC_MODEL_ATTITUDE: linearize_item<DMPC_MODEL_ATTITUDE>(s, xb, ub, t, d); break;
+      case DMPC_MODEL_CARTPOLE: linearize_item<DMPC_MODEL_CARTPOLE>(s, xb, ub, t, d); break;
+    }
+  }
+  __syncthreads();
+  const int nx = s.nx, nu = s.nu;
+  for (int w = threadIdx.x; w < s.K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    if (t == 0) {
+      s.C[i] = s.x0[i];
+    } else {
+      const int k = t - 1;
+      const double* Ar = s.A + ((size_t)k * nx + i) * nx;
+      const double* Br = s.Bm + ((size_t)k * nx + i) * nu;
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < nx; ++j) a += Ar[j] * xb[k * nx + j];
+      for (int j = 0; j < nu; ++j) b += Br[j] * ub[k * nu + j];
+      s.C[w] = -s.fv[k * nx + i] + a + b;
+    }
+  }
+}
+
+// Diagonal cost blocks (optimal_control_problem.py:249-323, sqp.py:160-197,243-244).
+// The Hessian of the weighted-square cost is 2 diag(w); PSD projection clamps its
+// eigenvalues at 1e-9 and q = J - x^T H uses the unprojected H.
+__device__ void linearize_cost(const Inst& s, const double* xb, const double* ub) {
+  const int nx = s.nx, nu = s.nu, N = s.N;
+  for (int w = threadIdx.x; w < s.K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    double h, ref;
+    if (t < N) {
+      h = 2.0 * s.wx[i];
+      ref = s.xref[t * nx + i];
+    } else {
+      h = 2.0 * (s.wx[i] + s.wf[i]);
+      ref = s.xf[i];
+    }
+    const double x = xb[w];
+    const double J = h * (x - ref);
+    s.q[w] = J - x * h;
+    s.Qi[w] = 1.0 / fmax(h, 1e-9);
+  }
+  for (int w = threadIdx.x; w < N * nu; w += blockDim.x) {
+    const int t = w / nu, i = w - t * nu;
+    const double h = 2.0 * s.wu[i];
+    const double ref = s.pen ? s.uref[t * nu + i] : 0.0;
+    const double u = ub[w];
+    const double J = h * (u - ref);
+    s.r[w] = J - u * h;
+    s.Ri[w] = 1.0 / fmax(h, 1e-9);
+  }
+}
+
+// ---------------------------------------------------------------- Schur assembly
+// theta_0 = Q0^-1; theta_{t+1} = A_t Q_t^-1 A_t^T + B_t R_t^-1 B_t^T + Q_{t+1}^-1;
+// phi_t = A_t Q_t^-1 An_{t-1}^T with An_{-1} = I, An = -I (pcg.py:182-196);
+// theta^-1 in FP64; P_t = -theta_t^-1 phi_{t-1} theta_{t-1}^-1 (pcg.py:213-239).
+// Writes FP64 blocks th/ph/ti/pm (row stride nx) and, for the mixed precision
+// path, FP32 copies with row stride ld.
+__device__ void assemble_schur(const Inst& s, bool fp32_copy) {
+  const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
+  const int nn = nx * nx;
+  for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
+    const int t = w / nn, e = w - t * nn, i = e / nx, j = e - i * nx;
+    double v;
+    if (t == 0) {
+      v = (i == j) ? s.Qi[i] : 0.0;
+    } else {
+      const int k = t - 1;
+      const double* Ai = s.A + ((size_t)k * nx + i) * nx;
+      const double* Aj = s.A + ((size_t)k * nx + j) * nx;
+      const double* Bi = s.Bm + ((size_t)k * nx + i) * nu;
+      const double* Bj = s.Bm + ((size_t)k * nx + j) * nu;
+      const double* D = s.Qi + k * nx;
+      const double* E = s.Ri + k * nu;
+      double a = 0.0, b = 0.0;
+      for (int l = 0; l < nx; ++l) a += Ai[l] * D[l] * Aj[l];
+      for (int l = 0; l < nu; ++l) b += Bi[l] * E[l] * Bj[l];
+      v = a + b + ((i == j) ? s.Qi[t * nx + i] : 0.0);
+    }
+    s.th[w] = v;
+    s.tmp[w] = v;
+    if (t < N) {
+      // phi_t = A_t D_t An_{t-1}^T : t == 0 -> A_0 D_0; t >= 1 -> -A_t D_t
+      const double ph = s.A[((size_t)t * nx + i) * nx + j] * s.Qi[t * nx + j];
+      s.ph[(size_t)t * nn + e] = (t == 0) ? ph : -ph;
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int t = warp; t < K; t += nwarp) warp_spd_inverse(s.tmp + (size_t)t * nn, s.ti + (size_t)t * nn, nx);
+  __syncthreads();
+  // T_t = theta_t^-1 phi_{t-1}  (t = 1..N), stored in tmp block t
+  for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
+    const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
+    const int t = k + 1;
+    const double* Ti = s.ti + (size_t)t * nn + i * nx;
+    const double* Pk = s.ph + (size_t)k * nn + j;
+    double a = 0.0;
+    for (int l = 0; l < nx; ++l) a += Ti[l] * Pk[l * nx];
+    s.tmp[(size_t)t * nn + e] = a;
+  }
+  __syncthreads();
+  // P_t = -T_t theta_{t-1}^-1, stored at index t-1
+  for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
+    const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
+    const int t = k + 1;
+    const double* Tr = s.tmp + (size_t)t * nn + i * nx;
+    const double* Tm = s.ti + (size_t)k * nn + j;
+    double a = 0.0;
+    for (int l = 0; l < nx; ++l) a += Tr[l] * Tm[l * nx];
+    s.pm[(size_t)k * nn + e] = -a;
+  }
+  if (fp32_copy) {
+    __syncthreads();
+    const int ld = s.ld;
+    for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
+      const int t = w / nn, e = w - t * nn, i = e / nx, j = e - i * nx;
+      const size_t o = ((size_t)t * nx + i) * ld + j;
+      s.th32[o] = (float)s.th[w];
+      s.ti32[o] = (float)s.ti[w];
+      if (t < N) {
+        s.ph32[o] = (float)s.ph[w];
+        s.pm32[o] = (float)s.pm[w];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// gamma = C + [Q0^-1 q0; A Q^-1 q + B R^-1 r + An Q_next^-1 q_next] (pcg.py:245-288),
+// with C == NULL meaning zeros (the adjoint, sqp.py:694-700).
+__device__ void compute_gamma(const Inst& s, const double* C, const double* q, const double* r) {
+  const int nx = s.nx, nu = s.nu;
+  for (int w = threadIdx.x; w < s.K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    double g;
+    if (t == 0) {
+      g = s.Qi[i] * q[i];
+    } else {
+      const int k = t - 1;
+      const double* Ar = s.A + ((size_t)k * nx + i) * nx;
+      const double* Br = s.Bm + ((size_t)k * nx + i) * nu;
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < nx; ++j) a += Ar[j] * (s.Qi[k * nx + j] * q[k * nx + j]);
+      for (int j = 0; j < nu; ++j) b += Br[j] * (s.Ri[k * nu + j] * r[k * nu + j]);
+      g = a + b - s.Qi[w] * q[w];
+    }
+    s.gam[w] = (C ? C[w] : 0.0) + g;
+  }
+}
+
+// ---------------------------------------------------------------- block-tridiagonal stencil
+// y_t = Off_{t-1} v_{t-1} + Dg_t v_t + Off_t^T v_{t+1}  for row (t, i) = g.
+template <class BT, class VT>
+__device__ __forceinline__ double stencil_row(const BT* Dg, const BT* Off, int ld, int nx, int N, const VT* v, int g) {
+  const int t = g / nx, i = g - t * nx;
+  const size_t bs = (size_t)nx * ld;
+  double acc;
+  {
+    const BT* row = Dg + t * bs + (size_t)i * ld;
+    const VT* vt = v + t * nx;
+    VT a = 0;
+    for (int j = 0; j < nx; ++j) a += (VT)row[j] * vt[j];
+    acc = (double)a;
+  }
+  if (t > 0) {
+    const BT* row = Off + (t - 1) * bs + (size_t)i * ld;
+    const VT* vm = v + (t - 1) * nx;
+    VT a = 0;
+    for (int j = 0; j < nx; ++j) a += (VT)row[j] * vm[j];
+    acc += (double)a;
+  }
+  if (t < N) {
+    const BT* col = Off + t * bs + i;
+    const VT* vp = v + (t + 1) * nx;
+    VT a = 0;
+    for (int j = 0; j < nx; ++j) a += (VT)col[(size_t)j * ld] * vp[j];
+    acc += (double)a;
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------- PCG, FP64 (reference recurrence)
+struct PcgOut {
+  int it;
+  double eta;
+};
+
+// Solves S lam = gam starting from lam (in/out, FP64 shared vector `lv`),
+// pcg.py:350-436: r = gamma - S lam; rt = Phi^-1 r; p = rt; eta = r.rt; loop while
+// (|eta| > eps && it <= max_iter - 1) || it < 1.
+__device__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, double* pv, double* tv, double* uv,
+                           int max_iter, double eps, double* red, int& par) {
+  const int n = s.K * s.nx, nx = s.nx, N = s.N;
+  double part = 0.0;
+  for (int g = threadIdx.x; g < n; g += blockDim.x)
+    rv[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lv, g);  // S = -stencil
+  __syncthreads();
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const double rt = stencil_row<double, double>(s.ti, s.pm, nx, nx, N, rv, g);
+    tv[g] = rt;
+    pv[g] = rt;
+    part += rv[g] * rt;
+  }
+  double eta = block_sum(part, red, par);
+  int it = 0;
+  while ((fabs(eta) > eps && it <= max_iter - 1) || it < 1) {
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const double u = -stencil_row<double, double>(s.th, s.ph, nx, nx, N, pv, g);
+      uv[g] = u;
+      part += pv[g] * u;
+    }
+    const double vden = block_sum(part, red, par);
+    const double alpha = eta / vden;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      lv[g] += alpha * pv[g];
+      rv[g] -= alpha * uv[g];
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const double rt = stencil_row<double, double>(s.ti, s.pm, nx, nx, N, rv, g);
+      tv[g] = rt;
+      part += rv[g] * rt;
+    }
+    const double etap = block_sum(part, red, par);
+    const double beta = etap / eta;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) pv[g] = tv[g] + beta * pv[g];
+    eta = etap;
+    ++it;
+    __syncthreads();
+  }
+  return PcgOut{it, eta};
+}
+
+// ---------------------------------------------------------------- PCG, FP32 + FP64 refinement
+// lam (FP64, workspace) in/out.  Outer loop: res = gamma - S64 lam, z = Phi64^-1 res,
+// eta64 = res.z; stop like the reference on eta64; otherwise solve S32 d = res/sqrt(eta64)
+// by FP32 PCG to a relative eta reduction of `inner_rel_tol` and update lam += d sqrt(eta64).
+__device__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, float* tv, float* uv, float* dv,
+                            int max_iter, double eps, int max_ref, double inner_rel, double* red, int& par) {
+  const int n = s.K * s.nx, nx = s.nx, N = s.N, ld = s.ld;
+  int it = 0;
+  double eta64 = 0.0;
+  for (int ref = 0;; ++ref) {
+    // FP64 residual and preconditioned norm
+    for (int g = threadIdx.x; g < n; g += blockDim.x)
+      s.res[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lam, g);
+    __syncthreads();
+    double part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x)
+      part += s.res[g] * stencil_row<double, double>(s.ti, s.pm, nx, nx, N, s.res, g);
+    eta64 = block_sum(part, red, par);
+    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
+    if (!cont || ref >= max_ref || !(eta64 == eta64)) break;
+    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+    // inner FP32 PCG on S32 d = res * scale, d0 = 0
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      rv[g] = (float)(s.res[g] * scale);
+      dv[g] = 0.0f;
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const float rt = (float)stencil_row<float, float>(s.ti32, s.pm32, ld, nx, N, rv, g);
+      tv[g] = rt;
+      pv[g] = rt;
+      part += (double)rv[g] * (double)rt;
+    }
+    double eta = block_sum(part, red, par);
+    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.25);
+    int inner = 0;
+    while ((eta > target && it <= max_iter - 1) || inner < 1) {
+      part = 0.0;
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const float u = -(float)stencil_row<float, float>(s.th32, s.ph32, ld, nx, N, pv, g);
+        uv[g] = u;
+        part += (double)pv[g] * (double)u;
+      }
+      const double vden = block_sum(part, red, par);
+      const float alpha = (float)(eta / vden);
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        dv[g] += alpha * pv[g];
+        rv[g] -= alpha * uv[g];
+      }
+      __syncthreads();
+      part = 0.0;
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const float rt = (float)stencil_row<float, float>(s.ti32, s.pm32, ld, nx, N, rv, g);
+        tv[g] = rt;
+        part += (double)rv[g] * (double)rt;
+      }
+      const double etap = block_sum(part, red, par);
+      const float beta = (float)(etap / eta);
+      for (int g = threadIdx.x; g < n; g += blockDim.x) pv[g] = tv[g] + beta * pv[g];
+      eta = etap;
+      ++it;
+      ++inner;
+      __syncthreads();
+      if (!(eta == eta) || !(vden == vden)) break;
+    }
+    const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) lam[g] += (double)dv[g] * back;
+    __syncthreads();
+  }
+  return PcgOut{it, eta64};
+}
+
+// ---------------------------------------------------------------- recovery (pcg.py:290-348)
+// x_t = -Qi_t (q_t + An_{t-1}^T lam_t + A_t^T lam_{t+1}), An_{-1} = I, An = -I;
+// u_t = -Ri_t (r_t + B_t^T lam_{t+1}); u_N = 0.
+__device__ void recover(const Inst& s, const double* lam, const double* q, const double* r, double* xo,
+                        double* uo, int ustride_rows) {
+  const int nx = s.nx, nu = s.nu, N = s.N;
+  for (int w = threadIdx.x; w < s.K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    double a = q[w] + ((t == 0) ? lam[w] : -lam[w]);
+    if (t < N) {
+      const double* Ac = s.A + (size_t)t * nx * nx + i;
+      const double* ln = lam + (t + 1) * nx;
+      double b = 0.0;
+      for (int j = 0; j < nx; ++j) b += Ac[(size_t)j * nx] * ln[j];
+      a += b;
+    }
+    xo[w] = -s.Qi[w] * a;
+  }
+  for (int w = threadIdx.x; w < ustride_rows * nu; w += blockDim.x) {
+    const int t = w / nu, i = w - t * nu;
+    if (t >= N) {
+      uo[w] = 0.0;
+      continue;
+    }
+    const double* Bc = s.Bm + (size_t)t * nx * nu + i;
+    const double* ln = lam + (t + 1) * nx;
+    double b = 0.0;
+    for (int j = 0; j < nx; ++j) b += Bc[(size_t)j * nu] * ln[j];
+    uo[w] = -s.Ri[w] * (r[w] + b);
+  }
+}
+
+// ---------------------------------------------------------------- line search (sqp.py:301-411)
+__device__ double stage_cost(const Inst& s, const double* x, const double* u) {
+  // per-thread partial of the reference cost (optimal_control_problem.py:208-247)
+  const int nx = s.nx, nu = s.nu, N = s.N;
+  double c = 0.0;
+  for (int w = threadIdx.x; w < s.K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    double d, wt;
+    if (t < N) {
+      d = x[w] - s.xref[t * nx + i];
+      wt = s.wx[i];
+    } else {
+      d = x[w] - s.xf[i];
+      wt = s.wx[i] + s.wf[i];
+    }
+    c += wt * d * d;
+  }
+  for (int w = threadIdx.x; w < N * nu; w += blockDim.x) {
+    const int t = w / nu, i = w - t * nu;
+    const double d = u[w] - (s.pen ? s.uref[t * nu + i] : 0.0);
+    c += s.wu[i] * d * d;
+  }
+  return c;
+}
+
+// returns the chosen alpha and overwrites xn/un with x + alpha (xn - x)
+__device__ double linesearch(const Inst& s, const dmpc_solver_params& P, const double* xb, const double* ub,
+                             double* xn, double* un, double* red, int& par, double* sh_dv) {
+  const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
+  // cost, directional derivative and constraint l1 at the current iterate
+  double c = stage_cost(s, xb, ub);
+  double cd = 0.0;
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    const double h = (t < N) ? 2.0 * s.wx[i] : 2.0 * (s.wx[i] + s.wf[i]);
+    const double ref = (t < N) ? s.xref[t * nx + i] : s.xf[i];
+    cd += h * (xb[w] - ref) * (xn[w] - xb[w]);
+  }
+  for (int w = threadIdx.x; w < N * nu; w += blockDim.x) {
+    const int t = w / nu, i = w - t * nu;
+    const double ref = s.pen ? s.uref[t * nu + i] : 0.0;
+    cd += 2.0 * s.wu[i] * (ub[w] - ref) * (un[w] - ub[w]);
+  }
+  double l1 = 0.0;
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    l1 += fabs((t == 0) ? (xb[i] - s.x0[i]) : (s.fv[(t - 1) * nx + i] - xb[w]));
+  }
+  const double cost = block_sum(c, red, par);
+  const double cdz = block_sum(cd, red, par);
+  const double l1n = block_sum(l1, red, par);
+  const double mu_min = cdz / (0.5 * l1n);
+  const double mu = (mu_min != mu_min) ? mu_min : fmax(0.1, mu_min);
+  const double merit = cost + mu * l1n;
+  const double merit_d = cdz + -mu * l1n;
+  const int na = P.n_alphas;
+  for (int a = 0; a < na; ++a) {
+    const double alpha = P.alphas[a];
+    double cc = 0.0, ll = 0.0;
+    // candidate cost
+    for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+      const int t = w / nx, i = w - t * nx;
+      const double x = xb[w] + alpha * (xn[w] - xb[w]);
+      const double d = x - ((t < N) ? s.xref[t * nx + i] : s.xf[i]);
+      cc += ((t < N) ? s.wx[i] : (s.wx[i] + s.wf[i])) * d * d;
+      if (t == 0) ll += fabs(x - s.x0[i]);
+    }
+    for (int w = threadIdx.x; w < N * nu; w += blockDim.x) {
+      const int t = w / nu, i = w - t * nu;
+      const double u = ub[w] + alpha * (un[w] - ub[w]);
+      const double d = u - (s.pen ? s.uref[t * nu + i] : 0.0);
+      cc += s.wu[i] * d * d;
+    }
+    // candidate dynamics defects: one integrator step per stage
+    for (int t = threadIdx.x; t < N; t += blockDim.x) {
+      double x[DMPC_MAX_NX], u[DMPC_MAX_NU], f[DMPC_MAX_NX];
+      for (int i = 0; i < nx; ++i) x[i] = xb[t * nx + i] + alpha * (xn[t * nx + i] - xb[t * nx + i]);
+      for (int i = 0; i < nu; ++i) u[i] = ub[t * nu + i] + alpha * (un[t * nu + i] - ub[t * nu + i]);
+      next_state_value(s, x, u, f);
+      for (int i = 0; i < nx; ++i) {
+        const int w = (t + 1) * nx + i;
+        ll += fabs(f[i] - (xb[w] + alpha * (xn[w] - xb[w])));
+      }
+    }
+    const double ccs = block_sum(cc, red, par);
+    const double lls = block_sum(ll, red, par);
+    if (threadIdx.x == 0) sh_dv[a] = ccs + mu * lls - (merit + P.linesearch_eta * alpha * merit_d);
+  }
+  __syncthreads();
+  // while_loop from index n+1 downwards with clamped gathers (sqp.py:389-403)
+  auto clampi = [&](int i) { return i < 0 ? 0 : (i > na - 1 ? na - 1 : i); };
+  double amax = P.alphas[0];
+  for (int a = 1; a < na; ++a) amax = fmax(amax, P.alphas[a]);
+  int i = na + 1;
+  double alpha = amax;
+  while (!(sh_dv[clampi(i)] < 0.0 || i == 0)) {
+    i = i - 1;
+    alpha = P.alphas[clampi(i)];
+  }
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) xn[w] = xb[w] + alpha * (xn[w] - xb[w]);
+  for (int w = threadIdx.x; w < K * nu; w += blockDim.x) un[w] = ub[w] + alpha * (un[w] - ub[w]);
+  __syncthreads();
+  return alpha;
+}
+
+// ---------------------------------------------------------------- grid mapping
+__device__ inline bool locate(const DevArgs& args, int b, int& gi, int& ii) {
+  for (int g = args.n_groups - 1; g >= 0; --g) {
+    if (b >= args.grp[g].first_block) {
+      gi = g;
+      ii = b - args.grp[g].first_block;
+      return ii < args.grp[g].g.batch;
+    }
+  }
+  return false;
+}
+
+__device__ inline double nan0(double v) {
+  // jnp.nan_to_num: NaN -> 0, +-inf -> +-max double
+  if (v != v) return 0.0;
+  if (v == __longlong_as_double(0x7ff0000000000000ll)) return 1.7976931348623157e308;
+  if (v == __longlong_as_double(0xfff0000000000000ll)) return -1.7976931348623157e308;
+  return v;
+}
+
+struct SmemView {
+  double* red;
+  double* dvals;  // line-search decrease values
+  void* vec;      // PCG vectors
+  float* blocks;  // FP32 blocks (if in smem)
+};
+
+__device__ inline SmemView carve_smem(unsigned char* sm, int nx, int K, int precision) {
+  SmemView v;
+  v.red = reinterpret_cast<double*>(sm);
+  v.dvals = v.red + 64;
+  unsigned char* p = sm + 64 * sizeof(double) + 64;
+  v.vec = p;
+  size_t vb = (precision == DMPC_PREC_FP64) ? 5 * (size_t)K * nx * sizeof(double)
+                                            : align_up(5 * (size_t)K * nx * sizeof(float), 16);
+  v.blocks = reinterpret_cast<float*>(p + vb);
+  return v;
+}
+
+// Solve the QP assembled in the workspace; lam (FP64 vector) in/out.
+__device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView& sv, double* lam, int& par) {
+  const int n = s.K * s.nx;
+  if (P.precision == DMPC_PREC_FP64) {
+    double* v = reinterpret_cast<double*>(sv.vec);
+    double *lv = v, *rv = v + n, *pv = v + 2 * n, *tv = v + 3 * n, *uv = v + 4 * n;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) lv[g] = lam[g];
+    __syncthreads();
+    PcgOut o = pcg_fp64(s, lv, rv, pv, tv, uv, P.pcg_max_iter, P.pcg_tol_epsilon, sv.red, par);
+    for (int g = threadIdx.x; g < n; g += blockDim.x) lam[g] = lv[g];
+    __syncthreads();
+    return o;
+  }
+  float* v = reinterpret_cast<float*>(sv.vec);
+  return pcg_mixed(s, lam, v, v + n, v + 2 * n, v + 3 * n, v + 4 * n, P.pcg_max_iter, P.pcg_tol_epsilon,
+                   P.max_refinement, P.inner_rel_tol, sv.red, par);
+}
+
+// ---------------------------------------------------------------- forward kernel
+__global__ void __launch_bounds__(512) k_sqp_fwd(const __grid_constant__ DevArgs args, void* ws) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int gi, ii;
+  if (!locate(args, blockIdx.x, gi, ii)) return;
+  const DevGroup& G = args.grp[gi];
+  const dmpc_group& g = G.g;
+  const dmpc_solver_params& P = args.p;
+  SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
+  Inst s = make_inst(G, ii, ws, sv.blocks);
+  const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K;
+  const int maxit = P.num_scp_iteration_max;
+  double* gx = g.states + (size_t)ii * Kmax * nx;
+  double* gu = g.controls + (size_t)ii * Kmax * nu;
+  double* gl = g.dual + (size_t)ii * Kmax * nx;
+  int par = 0;
+  // initial guess -> workspace
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    s.xb[w] = gx[w];
+    s.lam[w] = gl[w];
+  }
+  for (int w = threadIdx.x; w < K * nu; w += blockDim.x) s.ub[w] = gu[w];
+  __syncthreads();
+  double conv_err = g.convergence_error[ii];
+  int num_iter = 0;
+  const double tol = P.tol_convergence;
+  while ((num_iter < maxit && conv_err > tol) || num_iter < 1) {
+    // remember the linearization point of this iteration (used by the adjoint)
+    for (int w = threadIdx.x; w < K * nx; w += blockDim.x) g.lin_states[(size_t)ii * Kmax * nx + w] = s.xb[w];
+    for (int w = threadIdx.x; w < K * nu; w += blockDim.x) g.lin_controls[(size_t)ii * Kmax * nu + w] = s.ub[w];
+    linearize_dynamics(s, s.xb, s.ub);
+    linearize_cost(s, s.xb, s.ub);
+    __syncthreads();
+    assemble_schur(s, P.precision != DMPC_PREC_FP64);
+    compute_gamma(s, s.C, s.q, s.r);
+    __syncthreads();
+    PcgOut o = solve_qp(s, P, sv, s.lam, par);
+    recover(s, s.lam, s.q, s.r, s.xn, s.un, K);
+    __syncthreads();
+    double alpha = 0.0;
+    if (P.linesearch) alpha = linesearch(s, P, s.xb, s.ub, s.xn, s.un, sv.red, par, sv.dvals);
+    double e = 0.0;
+    for (int w = threadIdx.x; w < K * nx; w += blockDim.x) e = fmax(e, fabs(s.xn[w] - s.xb[w]));
+    for (int w = threadIdx.x; w < K * nu; w += blockDim.x) e = fmax(e, fabs(s.un[w] - s.ub[w]));
+    // NaN-propagating max like jnp.max
+    {
+      double ee = 0.0;
+      bool nan = false;
+      for (int w = threadIdx.x; w < K * nx; w += blockDim.x) nan |= (s.xn[w] != s.xn[w]) || (s.xb[w] != s.xb[w]);
+      for (int w = threadIdx.x; w < K * nu; w += blockDim.x) nan |= (s.un[w] != s.un[w]) || (s.ub[w] != s.ub[w]);
+      ee = nan ? __longlong_as_double(0x7ff8000000000000ll) : e;
+      conv_err = block_max(ee, sv.red, par);
+    }
+    if (threadIdx.x == 0 && num_iter < maxit) {
+      g.convergence_errors[(size_t)ii * maxit + num_iter] = conv_err;
+      g.num_pcg_iters[(size_t)ii * maxit + num_iter] = o.it;
+      if (P.linesearch) g.linesearch_alphas[(size_t)ii * maxit + num_iter] = alpha;
+    }
+    for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.xb[w] = s.xn[w];
+    for (int w = threadIdx.x; w < K * nu; w += blockDim.x) s.ub[w] = s.un[w];
+    ++num_iter;
+    __syncthreads();
+  }
+  // status + nan_to_num (sqp.py:535-559)
+  bool nan = false;
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) nan |= (s.xb[w] != s.xb[w]);
+  for (int w = threadIdx.x; w < K * nu; w += blockDim.x) nan |= (s.ub[w] != s.ub[w]);
+  const int anynan = __syncthreads_or(nan ? 1 : 0);
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    gx[w] = nan0(s.xb[w]);
+    gl[w] = nan0(s.lam[w]);
+  }
+  for (int w = threadIdx.x; w < K * nu; w += blockDim.x) gu[w] = nan0(s.ub[w]);
+  if (threadIdx.x == 0) {
+    g.status[ii] = (anynan || conv_err > tol || conv_err != conv_err) ? DMPC_STATUS_ERROR : DMPC_STATUS_SUCCESS;
+    g.num_iter[ii] = num_iter;
+    g.convergence_error[ii] = conv_err;
+  }
+}
+
+// ---------------------------------------------------------------- adjoint kernel
+// Hyper-dual evaluation for model-parameter gradients: the e1e2 part of
+// lam*_{t+1} . F(z*_t + z~_t e1, theta + e_k e2) and the e2 part against lam~_{t+1}.
+template <int MODEL>
+__device__ double param_grad_item(const Inst& s, const double* xs, const double* us, const double* xt,
+                                  const double* ut, const double* lstar, const double* ltil, int t, int k) {
+  constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
+  const int nx = s.nx, nu = s.nu;
+  HDual x[MX], u[MU], f[MX];
+  for (int j = 0; j < nx; ++j) x[j] = HDual(xs[t * nx + j], xt[t * nx + j], 0.0, 0.0);
+  for (int j = 0; j < nu; ++j) u[j] = HDual(us[t * nu + j], ut[t * nu + j], 0.0, 0.0);
+  if (MODEL == DMPC_MODEL_LINEAR) {
+    predict_next_state_linear<HDual>(s, x, u, f, k);
+  } else {
+    HDual p[12];
+    for (int q = 0; q < s.P && q < 12; ++q) p[q] = HDual(s.mp[q], 0.0, q == k ? 1.0 : 0.0, 0.0);
+    predict_next_state<HDual, MODEL>(s.scheme, s.dt, nx, nu, x, u, p, f);
+  }
+  double acc = 0.0;
+  for (int i = 0; i < nx; ++i) acc += lstar[(t + 1) * nx + i] * f[i].ab + ltil[(t + 1) * nx + i] * f[i].b;
+  return acc;
+}
+
+__global__ void __launch_bounds__(512) k_sqp_adj(const __grid_constant__ DevArgs args, void* ws) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int gi, ii;
+  if (!locate(args, blockIdx.x, gi, ii)) return;
+  const DevGroup& G = args.grp[gi];
+  const dmpc_group& g = G.g;
+  const dmpc_adjoint& a = G.a;
+  const dmpc_solver_params& P = args.p;
+  SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
+  Inst s = make_inst(G, ii, ws, sv.blocks);
+  const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K, N = s.N;
+  const size_t ox = (size_t)ii * Kmax * nx, ou = (size_t)ii * Kmax * nu;
+  int par = 0;
+  // linearization point of the last SQP iteration (sqp.py:761-763)
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.xb[w] = g.lin_states[ox + w];
+  for (int w = threadIdx.x; w < K * nu; w += blockDim.x) s.ub[w] = g.lin_controls[ou + w];
+  __syncthreads();
+  linearize_dynamics(s, s.xb, s.ub);
+  linearize_cost(s, s.xb, s.ub);
+  // q = -dl/dx, r = -dl/du[:-1] (sqp.py:682-683)
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.q[w] = -a.dl_dstates[ox + w];
+  for (int w = threadIdx.x; w < N * nu; w += blockDim.x) s.r[w] = -a.dl_dcontrols[ou + w];
+  __syncthreads();
+  assemble_schur(s, P.precision != DMPC_PREC_FP64);
+  compute_gamma(s, nullptr, s.q, s.r);
+  const bool warm = P.warm_start_backward && a.dual_backward_guess;
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.lam[w] = warm ? a.dual_backward_guess[ox + w] : 0.0;
+  __syncthreads();
+  PcgOut o = solve_qp(s, P, sv, s.lam, par);
+  // adjoint states/controls (x~, u~)
+  recover(s, s.lam, s.q, s.r, s.xn, s.un, K);
+  __syncthreads();
+  const double* xs = g.states + ox;  // z*, lambda* (post nan_to_num)
+  const double* us = g.controls + ou;
+  const double* ls = g.dual + ox;
+  const double* xt = s.xn;
+  const double* ut = s.un;
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    a.dual_backward[ox + w] = s.lam[w];
+    if (a.adj_states) a.adj_states[ox + w] = xt[w];
+  }
+  if (a.adj_controls)
+    for (int w = threadIdx.x; w < K * nu; w += blockDim.x) a.adj_controls[ou + w] = ut[w];
+  if (threadIdx.x == 0 && a.num_pcg_iter) a.num_pcg_iter[ii] = o.it;
+  // closed-form gradients of the cost-related parameters (sqp.py:605-666,724-739)
+  const int j = threadIdx.x;
+  if (j < nx) {
+    double gwx = 0.0;
+    for (int t = 0; t < N; ++t) gwx += 2.0 * (xs[t * nx + j] - s.xref[t * nx + j]) * xt[t * nx + j];
+    const double dN = xs[N * nx + j] - s.xf[j];
+    const double xtN = xt[N * nx + j];
+    gwx += 2.0 * dN * xtN;
+    if (a.g_w_x) a.g_w_x[(size_t)ii * nx + j] = -gwx;
+    if (a.g_w_f) a.g_w_f[(size_t)ii * nx + j] = -2.0 * dN * xtN;
+    if (a.g_initial_state) a.g_initial_state[(size_t)ii * nx + j] = s.lam[j];
+    if (a.g_final_state) a.g_final_state[(size_t)ii * nx + j] = 2.0 * (s.wx[j] + s.wf[j]) * xtN;
+  } else if (j < nx + nu) {
+    const int k = j - nx;
+    double gwu = 0.0;
+    for (int t = 0; t < N; ++t)
+      gwu += 2.0 * (us[t * nu + k] - (s.pen ? s.uref[t * nu + k] : 0.0)) * ut[t * nu + k];
+    if (a.g_w_u) a.g_w_u[(size_t)ii * nu + k] = -gwu;
+  }
+  if (a.g_reference_state)
+    for (int w = threadIdx.x; w < Kmax * nx; w += blockDim.x) {
+      const int t = w / nx, i = w - t * nx;
+      a.g_reference_state[ox + w] = (t < N) ? 2.0 * s.wx[i] * xt[w] : 0.0;
+    }
+  if (a.g_reference_control)
+    for (int w = threadIdx.x; w < Kmax * nu; w += blockDim.x) {
+      const int t = w / nu, i = w - t * nu;
+      a.g_reference_control[ou + w] = (t < N && s.pen) ? 2.0 * s.wu[i] * ut[w] : 0.0;
+    }
+  // model parameters: hyper-dual mixed partials through the integrator
+  const int ng = a.n_param_grads;
+  if (ng > 0 && a.g_model_params) {
+    for (int w = threadIdx.x; w < N * ng; w += blockDim.x) {
+      const int t = w / ng, q = w - t * ng;
+      const int k = G.pg_idx[q];
+      double v = 0.0;
+      switch (s.model) {
+        case DMPC_MODEL_LINEAR: v = param_grad_item<DMPC_MODEL_LINEAR>(s, xs, us, xt, ut, ls, s.lam, t, k); break;
+        case DMPC_MODEL_QUADROTOR: v = param_grad_item<DMPC_MODEL_QUADROTOR>(s, xs, us, xt, ut, ls, s.lam, t, k); break;
+        case DMPC_MODEL_SPACECRAFT: v = param_grad_item<DMPC_MODEL_SPACECRAFT>(s, xs, us, xt, ut, ls, s.lam, t, k); break;
+        case DMPC_MODEL_ATTITUDE: v = param_grad_item<DMPC_MODEL_ATTITUDE>(s, xs, us, xt, ut, ls, s.lam, t, k); break;
+        case DMPC_MODEL_CARTPOLE: v = param_grad_item<DMPC_MODEL_CARTPOLE>(s, xs, us, xt, ut, ls, s.lam, t, k); break;
+      }
+      s.contrib[(size_t)q * K + t] = v;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < ng; q += blockDim.x) {
+      double acc = 0.0;
+      for (int t = 0; t < N; ++t) acc += s.contrib[(size_t)q * K + t];
+      a.g_model_params[(size_t)ii * ng + q] = -acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- dense-layout parity kernels
+// dmpc_linearize: dense As, Bs, Cs, Qinv, qvec, Rinv, rvec of one group
+__global__ void __launch_bounds__(256) k_linearize(const __grid_constant__ DevArgs args, void* ws, double* As,
+                                                   double* Bs, double* Cs, double* Qinv, double* qv, double* Rinv,
+                                                   double* rv) {
+  int gi, ii;
+  if (!locate(args, blockIdx.x, gi, ii)) return;
+  const DevGroup& G = args.grp[gi];
+  const dmpc_group& g = G.g;
+  Inst s = make_inst(G, ii, ws, nullptr);
+  const int nx = s.nx, nu = s.nu, N = G.g.horizon, K = N + 1;
+  const double* xb = g.states + (size_t)ii * K * nx;
+  const double* ub = g.controls + (size_t)ii * K * nu;
+  linearize_dynamics(s, xb, ub);
+  linearize_cost(s, xb, ub);
+  __syncthreads();
+  for (int w = threadIdx.x; w < N * nx * nx; w += blockDim.x) As[(size_t)ii * N * nx * nx + w] = s.A[w];
+  for (int w = threadIdx.x; w < N * nx * nu; w += blockDim.x) Bs[(size_t)ii * N * nx * nu + w] = s.Bm[w];
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    Cs[(size_t)ii * K * nx + w] = s.C[w];
+    qv[(size_t)ii * K * nx + w] = s.q[w];
+  }
+  for (int w = threadIdx.x; w < K * nx * nx; w += blockDim.x) {
+    const int t = w / (nx * nx), e = w - t * nx * nx, i = e / nx, j = e - i * nx;
+    Qinv[(size_t)ii * K * nx * nx + w] = (i == j) ? s.Qi[t * nx + i] : 0.0;
+  }
+  for (int w = threadIdx.x; w < N * nu * nu; w += blockDim.x) {
+    const int t = w / (nu * nu), e = w - t * nu * nu, i = e / nu, j = e - i * nu;
+    Rinv[(size_t)ii * N * nu * nu + w] = (i == j) ? s.Ri[t * nu + i] : 0.0;
+  }
+  for (int w = threadIdx.x; w < N * nu; w += blockDim.x) rv[(size_t)ii * N * nu + w] = s.r[w];
+}
+
+// dmpc_schur_assemble: general QP data (any As_next, dense Qinv / Rinv), FP64
+__global__ void __launch_bounds__(256) k_schur_dense(int N, int nx, int nu, const double* As_next, const double* As,
+                                                     const double* Bs, const double* Cs, const double* Qinv,
+                                                     const double* qvec, const double* Rinv, const double* rvec,
+                                                     double* S, double* Phiinv, double* gamma, double* ws) {
+  const int b = blockIdx.x, K = N + 1, nn = nx * nx;
+  const double* An = As_next + (size_t)b * N * nn;
+  const double* A = As + (size_t)b * N * nn;
+  const double* B = Bs + (size_t)b * N * nx * nu;
+  const double* Qi = Qinv + (size_t)b * K * nn;
+  const double* Ri = Rinv + (size_t)b * N * nu * nu;
+  double* th = ws + (size_t)b * 4 * K * nn;
+  double* ph = th + K * nn;
+  double* ti = ph + K * nn;
+  double* tm = ti + K * nn;
+  // theta, phi
+  for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
+    const int t = w / nn, e = w - t * nn, i = e / nx, j = e - i * nx;
+    double v;
+    if (t == 0) {
+      v = Qi[e];
+    } else {
+      const int k = t - 1;
+      const double* Ak = A + (size_t)k * nn;
+      const double* Ank = An + (size_t)k * nn;
+      const double* Bk = B + (size_t)k * nx * nu;
+      const double* Q0 = Qi + (size_t)k * nn;
+      const double* Q1 = Qi + (size_t)(k + 1) * nn;
+      const double* R0 = Ri + (size_t)k * nu * nu;
+      v = 0.0;
+      for (int l = 0; l < nx; ++l)
+        for (int m = 0; m < nx; ++m) v += Ak[i * nx + l] * Q0[l * nx + m] * Ak[j * nx + m];
+      for (int l = 0; l < nu; ++l)
+        for (int m = 0; m < nu; ++m) v += Bk[i * nu + l] * R0[l * nu + m] * Bk[j * nu + m];
+      for (int l = 0; l < nx; ++l)
+        for (int m = 0; m < nx; ++m) v += Ank[i * nx + l] * Q1[l * nx + m] * Ank[j * nx + m];
+    }
+    th[w] = v;
+    tm[w] = v;
+    if (t < N) {
+      // phi_t = A_t Qinv_t Anext_{t-1}^T, Anext_{-1} = I
+      const double* Ak = A + (size_t)t * nn;
+      const double* Q0 = Qi + (size_t)t * nn;
+      double p = 0.0;
+      for (int l = 0; l < nx; ++l)
+        for (int m = 0; m < nx; ++m) {
+          const double anp = (t == 0) ? ((j == m) ? 1.0 : 0.0) : An[(size_t)(t - 1) * nn + j * nx + m];
+          p += Ak[i * nx + l] * Q0[l * nx + m] * anp;
+        }
+      ph[(size_t)t * nn + e] = p;
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int t = warp; t < K; t += nwarp) warp_spd_inverse(tm + (size_t)t * nn, ti + (size_t)t * nn, nx);
+  __syncthreads();
+  // S and Phiinv rows (pcg.py:198-239)
+  const int rw = 3 * nx;
+  for (int w = threadIdx.x; w < K * nx * rw; w += blockDim.x) {
+    const int t = w / (nx * rw), e = w - t * nx * rw, i = e / rw, c = e - i * rw;
+    const int blk = c / nx, j = c - blk * nx;
+    double sv = 0.0, pv = 0.0;
+    if (blk == 1) {
+      sv = -th[(size_t)t * nn + i * nx + j];
+      pv = ti[(size_t)t * nn + i * nx + j];
+    } else if (blk == 0 && t > 0) {
+      const double* phm = ph + (size_t)(t - 1) * nn;
+      sv = -phm[i * nx + j];
+      // -theta_t^-1 phi_{t-1} theta_{t-1}^-1
+      const double* Ti = ti + (size_t)t * nn;
+      const double* Tm = ti + (size_t)(t - 1) * nn;
+      double acc = 0.0;
+      for (int l = 0; l < nx; ++l) {
+        double m = 0.0;
+        for (int o = 0; o < nx; ++o) m += Ti[i * nx + o] * phm[o * nx + l];
+        acc += m * Tm[l * nx + j];
+      }
+      pv = -acc;
+    } else if (blk == 2 && t < N) {
+      const double* pht = ph + (size_t)t * nn;
+      sv = -pht[j * nx + i];
+      // -theta_t^-1 phi_t^T theta_{t+1}^-1
+      const double* Ti = ti + (size_t)t * nn;
+      const double* Tp = ti + (size_t)(t + 1) * nn;
+      double acc = 0.0;
+      for (int l = 0; l < nx; ++l) {
+        double m = 0.0;
+        for (int o = 0; o < nx; ++o) m += Ti[i * nx + o] * pht[l * nx + o];
+        acc += m * Tp[l * nx + j];
+      }
+      pv = -acc;
+    }
+    S[(size_t)b * K * nx * rw + w] = sv;
+    Phiinv[(size_t)b * K * nx * rw + w] = pv;
+  }
+  // gamma
+  const double* q = qvec + (size_t)b * K * nx;
+  const double* r = rvec + (size_t)b * N * nu;
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) {
+    const int t = w / nx, i = w - t * nx;
+    double gv = 0.0;
+    if (t == 0) {
+      for (int l = 0; l < nx; ++l) gv += Qi[i * nx + l] * q[l];
+    } else {
+      const int k = t - 1;
+      const double* Ak = A + (size_t)k * nn;
+      const double* Ank = An + (size_t)k * nn;
+      const double* Bk = B + (size_t)k * nx * nu;
+      const double* Q0 = Qi + (size_t)k * nn;
+      const double* Q1 = Qi + (size_t)t * nn;
+      const double* R0 = Ri + (size_t)k * nu * nu;
+      for (int l = 0; l < nx; ++l) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int m = 0; m < nx; ++m) {
+          a0 += Q0[l * nx + m] * q[k * nx + m];
+          a1 += Q1[l * nx + m] * q[t * nx + m];
+        }
+        gv += Ak[i * nx + l] * a0 + Ank[i * nx + l] * a1;
+      }
+      for (int l = 0; l < nu; ++l) {
+        double a0 = 0.0;
+        for (int m = 0; m < nu; ++m) a0 += R0[l * nu + m] * r[k * nu + m];
+        gv += Bk[i * nu + l] * a0;
+      }
+    }
+    gamma[(size_t)b * K * nx + w] = Cs[(size_t)b * K * nx + w] + gv;
+  }
+}
+
+// dense 3-block stencil row: y = M_t [v_{t-1}; v_t; v_{t+1}]
+__device__ inline double dense_row(const double* M, const double* v, int nx, int N, int g) {
+  const int t = g / nx, i = g - t * nx;
+  const double* row = M + ((size_t)t * nx + i) * 3 * nx;
+  double a = 0.0;
+  for (int blk = 0; blk < 3; ++blk) {
+    const int tt = t + blk - 1;
+    if (tt < 0 || tt > N) continue;
+    for (int j = 0; j < nx; ++j) a += row[blk * nx + j] * v[tt * nx + j];
+  }
+  return a;
+}
+
+// x_t = -Qinv_t (q_t + An_{t-1}^T lam_t + A_t^T lam_{t+1}), An_{-1} = I,
+// x_N = -Qinv_N (q_N + An_{N-1}^T lam_N), u_t = -Rinv_t (r_t + B_t^T lam_{t+1}), u_N = 0
+// (pcg.py:290-348), general dense matrices.  `tv` is K*nx scratch.
+__device__ void dense_recover(int b, int N, int nx, int nu, const double* lv, double* tv, const double* As_next,
+                              const double* As, const double* Bs, const double* Qinv, const double* qvec,
+                              const double* Rinv, const double* rvec, double* xs, double* us) {
+  const int K = N + 1, n = K * nx, nn = nx * nx;
+  const double* An = As_next + (size_t)b * N * nn;
+  const double* A = As + (size_t)b * N * nn;
+  const double* B = Bs + (size_t)b * N * nx * nu;
+  const double* Qi = Qinv + (size_t)b * K * nn;
+  const double* Ri = Rinv + (size_t)b * N * nu * nu;
+  const double* q = qvec + (size_t)b * n;
+  const double* r = rvec + (size_t)b * N * nu;
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx, i = g - t * nx;
+    double a = q[g];
+    if (t == 0) {
+      a += lv[i];
+    } else {
+      const double* Ap = An + (size_t)(t - 1) * nn;
+      for (int j = 0; j < nx; ++j) a += Ap[j * nx + i] * lv[t * nx + j];
+    }
+    if (t < N) {
+      const double* At = A + (size_t)t * nn;
+      for (int j = 0; j < nx; ++j) a += At[j * nx + i] * lv[(t + 1) * nx + j];
+    }
+    tv[g] = a;
+  }
+  __syncthreads();
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx, i = g - t * nx;
+    const double* Qt = Qi + (size_t)t * nn + i * nx;
+    double a = 0.0;
+    for (int j = 0; j < nx; ++j) a += Qt[j] * tv[t * nx + j];
+    xs[(size_t)b * n + g] = -a;
+  }
+  for (int g = threadIdx.x; g < K * nu; g += blockDim.x) {
+    const int t = g / nu, i = g - t * nu;
+    double val = 0.0;
+    if (t < N) {
+      const double* Bt = B + (size_t)t * nx * nu;
+      const double* Rt = Ri + (size_t)t * nu * nu + i * nu;
+      for (int m = 0; m < nu; ++m) {
+        double c = r[t * nu + m];
+        for (int j = 0; j < nx; ++j) c += Bt[j * nu + m] * lv[(t + 1) * nx + j];
+        val += Rt[m] * c;
+      }
+      val = -val;
+    }
+    us[(size_t)b * K * nu + g] = val;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_recover_dense(int N, int nx, int nu, const double* lam, const double* As_next,
+                                                       const double* As, const double* Bs, const double* Qinv,
+                                                       const double* qvec, const double* Rinv, const double* rvec,
+                                                       double* xs, double* us) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int b = blockIdx.x, n = (N + 1) * nx;
+  double* lv = reinterpret_cast<double*>(smem);
+  double* tv = lv + n;
+  for (int g = threadIdx.x; g < n; g += blockDim.x) lv[g] = lam[(size_t)b * n + g];
+  __syncthreads();
+  dense_recover(b, N, nx, nu, lv, tv, As_next, As, Bs, Qinv, qvec, Rinv, rvec, xs, us);
+}
+
+// gamma from the premultiplied matrices (pcg.py:245-288)
+__global__ void __launch_bounds__(256) k_gamma_dense(int N, int nx, int nu, const double* AQ, const double* AnQ,
+                                                     const double* BR, const double* Cs, const double* Q0inv,
+                                                     const double* qs, const double* rs, double* gamma) {
+  const int b = blockIdx.x, K = N + 1, n = K * nx, nn = nx * nx;
+  const double* q = qs + (size_t)b * n;
+  const double* r = rs + (size_t)b * N * nu;
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx, i = g - t * nx;
+    double v = 0.0;
+    if (t == 0) {
+      const double* Q0 = Q0inv + (size_t)b * nn + i * nx;
+      for (int j = 0; j < nx; ++j) v += Q0[j] * q[j];
+    } else {
+      const int k = t - 1;
+      const double* a = AQ + ((size_t)b * N + k) * nn + i * nx;
+      const double* an = AnQ + ((size_t)b * N + k) * nn + i * nx;
+      const double* br = BR + ((size_t)b * N + k) * nx * nu + i * nu;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      for (int j = 0; j < nx; ++j) s0 += a[j] * q[k * nx + j];
+      for (int j = 0; j < nu; ++j) s1 += br[j] * r[k * nu + j];
+      for (int j = 0; j < nx; ++j) s2 += an[j] * q[t * nx + j];
+      v = s0 + s1 + s2;
+    }
+    gamma[(size_t)b * n + g] = Cs[(size_t)b * n + g] + v;
+  }
+}
+
+// dmpc_pcg_solve: solve_KKT_Schur on the dense layout (pcg.py:350-445), FP64
+__global__ void __launch_bounds__(256) k_pcg_dense(int N, int nx, int nu, const double* S, const double* Phi,
+                                                   const double* gamma, const double* lam0, const double* As_next,
+                                                   const double* As, const double* Bs, const double* Qinv,
+                                                   const double* qvec, const double* Rinv, const double* rvec,
+                                                   int max_iter, double eps, double* lam_out, double* xs,
+                                                   double* us, int32_t* iters, double* etas) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int b = blockIdx.x, K = N + 1, n = K * nx, nn = nx * nx;
+  double* red = reinterpret_cast<double*>(smem);
+  double* lv = red + 64;
+  double *rv = lv + n, *pv = rv + n, *tv = pv + n, *uv = tv + n;
+  const double* Sb = S + (size_t)b * K * nx * 3 * nx;
+  const double* Pb = Phi + (size_t)b * K * nx * 3 * nx;
+  const double* gb = gamma + (size_t)b * n;
+  int par = 0;
+  for (int g = threadIdx.x; g < n; g += blockDim.x) lv[g] = lam0[(size_t)b * n + g];
+  __syncthreads();
+  for (int g = threadIdx.x; g < n; g += blockDim.x) rv[g] = gb[g] - dense_row(Sb, lv, nx, N, g);
+  __syncthreads();
+  double part = 0.0;
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const double rt = dense_row(Pb, rv, nx, N, g);
+    tv[g] = rt;
+    pv[g] = rt;
+    part += rv[g] * rt;
+  }
+  double eta = block_sum(part, red, par);
+  int it = 0;
+  while ((fabs(eta) > eps && it <= max_iter - 1) || it < 1) {
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const double u = dense_row(Sb, pv, nx, N, g);
+      uv[g] = u;
+      part += pv[g] * u;
+    }
+    const double vden = block_sum(part, red, par);
+    const double alpha = eta / vden;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      lv[g] += alpha * pv[g];
+      rv[g] -= alpha * uv[g];
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const double rt = dense_row(Pb, rv, nx, N, g);
+      tv[g] = rt;
+      part += rv[g] * rt;
+    }
+    const double etap = block_sum(part, red, par);
+    const double beta = etap / eta;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) pv[g] = tv[g] + beta * pv[g];
+    eta = etap;
+    ++it;
+    __syncthreads();
+  }
+  for (int g = threadIdx.x; g < n; g += blockDim.x) lam_out[(size_t)b * n + g] = lv[g];
+  __syncthreads();
+  dense_recover(b, N, nx, nu, lv, tv, As_next, As, Bs, Qinv, qvec, Rinv, rvec, xs, us);
+  if (threadIdx.x == 0) {
+    iters[b] = it;
+    etas[b] = eta;
+  }
+}
+
+// ---------------------------------------------------------------- FP32 FMA throughput probe
+// Eight independent FMA chains per thread; used only to measure the FP32 CUDA-core
+// peak that serves as the roofline denominator of the (shared-memory resident) PCG.
+__global__ void __launch_bounds__(256) k_fma_probe(int iters, float seed, float* out) {
+  float a0 = seed + threadIdx.x, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+  float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+  const float m = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+      a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+    }
+  }
+  const float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 12345.678f) out[blockIdx.x] = r;  // keeps the chains live
+}
+
+// ---------------------------------------------------------------- host side
+int choose_threads(const dmpc_solver_params* p, int nx, int K) {
+  if (p && p->threads_per_block > 0) return p->threads_per_block;
+  const int rows = K * nx;
+  int t = ((rows + 31) / 32) * 32;
+  if (t < 128) t = 128;
+  if (t > 512) t = 512;
+  return t;
+}
+
+int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, const dmpc_solver_params* p,
+              DevArgs* args, size_t* ws_total, size_t* smem_max, int* threads) {
+  if (n_groups < 1 || n_groups > kMaxGroups || !groups || !p) return DMPC_ERR_INVALID;
+  if (p->precision != DMPC_PREC_FP64 && p->precision != DMPC_PREC_MIXED) return DMPC_ERR_INVALID;
+  if (p->n_alphas < 1 || p->n_alphas > DMPC_MAX_ALPHAS) return DMPC_ERR_INVALID;
+  if (p->threads_per_block != 0 &&
+      (p->threads_per_block < 64 || p->threads_per_block > 512 || (p->threads_per_block & 31) != 0))
+    return DMPC_ERR_INVALID;
+  if (p->num_scp_iteration_max < 1 || p->pcg_max_iter < 1 || p->max_refinement < 1) return DMPC_ERR_INVALID;
+  memset(args, 0, sizeof(DevArgs));
+  args->n_groups = n_groups;
+  args->p = *p;
+  size_t off = 0, smax = 0;
+  int blocks = 0, thr = 0;
+  int dev = 0;
+  int smem_optin = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (smem_optin <= 0) smem_optin = 227 * 1024;
+  for (int k = 0; k < n_groups; ++k) {
+    const dmpc_group& g = groups[k];
+    if (!model_dims_ok(g.model, g.nx, g.nu)) return DMPC_ERR_UNSUPPORTED;
+    if (g.horizon < 1 || g.batch < 0 || g.scheme < 0 || g.scheme > 2) return DMPC_ERR_INVALID;
+    if (g.n_model_params != model_param_count(g.model, g.nx, g.nu)) return DMPC_ERR_INVALID;
+    DevGroup& G = args->grp[k];
+    G.g = g;
+    if (adj) G.a = adj[k];
+    G.first_block = blocks;
+    G.K = g.horizon + 1;
+    G.ld32 = odd_ld(g.nx);
+    const size_t need_smem_blocks = smem_bytes_for(g.nx, g.horizon, p->precision, true);
+    bool in_smem = (p->precision == DMPC_PREC_MIXED) && (size_t)need_smem_blocks <= (size_t)smem_optin;
+    if (p->blocks_in_smem == 0) in_smem = false;
+    if (p->blocks_in_smem == 1 && p->precision == DMPC_PREC_MIXED && !in_smem) return DMPC_ERR_UNSUPPORTED;
+    G.blocks_smem = in_smem ? 1 : 0;
+    const size_t sm = smem_bytes_for(g.nx, g.horizon, p->precision, in_smem);
+    if (sm > (size_t)smem_optin) return DMPC_ERR_UNSUPPORTED;
+    if (sm > smax) smax = sm;
+    int ng = 0;
+    if (adj) {
+      ng = adj[k].n_param_grads;
+      if (ng < 0 || ng > g.n_model_params || ng > DMPC_MAX_PARAM_GRADS) return DMPC_ERR_INVALID;
+      for (int q = 0; q < ng; ++q) {
+        const int idx = adj[k].param_grad_index[q];
+        if (idx < 0 || idx >= g.n_model_params) return DMPC_ERR_INVALID;
+        G.pg_idx[q] = idx;
+      }
+    } else {
+      ng = g.n_model_params;  // size the workspace for any later adjoint call
+    }
+    Layout L = make_layout(g.nx, g.nu, g.horizon, G.ld32, !in_smem, g.n_model_params);
+    G.ws_offset = off;
+    G.ws_stride = L.bytes;
+    off += L.bytes * (size_t)g.batch;
+    blocks += g.batch;
+    const int t = choose_threads(p, g.nx, G.K);
+    if (t > thr) thr = t;
+  }
+  args->total_blocks = blocks;
+  *ws_total = off;
+  *smem_max = smax;
+  *threads = thr;
+  return DMPC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmpc_abi_version(void) { return DMPC_ABI_VERSION; }
+
+const char* dmpc_error_string(int code) {
+  switch (code) {
+    case DMPC_OK: return "ok";
+    case DMPC_ERR_INVALID: return "invalid descriptor or sizes";
+    case DMPC_ERR_WORKSPACE: return "workspace too small or misaligned";
+    case DMPC_ERR_CUDA: return "CUDA runtime error";
+    case DMPC_ERR_UNSUPPORTED: return "unsupported model or option";
+  }
+  return "unknown error";
+}
+
+void dmpc_default_params(dmpc_solver_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->tol_convergence = 1e-8;
+  p->num_scp_iteration_max = 15;
+  p->linesearch = 0;
+  p->linesearch_eta = 0.4;
+  p->n_alphas = 5;
+  const double al[5] = {0.01, 0.1, 0.3, 0.7, 1.0};
+  for (int i = 0; i < 5; ++i) p->alphas[i] = al[i];
+  p->warm_start_backward = 1;
+  p->pcg_max_iter = 10000;
+  p->pcg_tol_epsilon = 1e-9;
+  p->precision = DMPC_PREC_MIXED;
+  p->max_refinement = 12;
+  p->inner_rel_tol = 1e-8;
+  p->threads_per_block = 0;
+  p->blocks_in_smem = -1;
+}
+
+size_t dmpc_workspace_size(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params) {
+  DevArgs* a = new DevArgs;
+  size_t ws = 0, sm = 0;
+  int thr = 0;
+  int rc = fill_args(n_groups, groups, nullptr, params, a, &ws, &sm, &thr);
+  delete a;
+  return rc == DMPC_OK ? ws : 0;
+}
+
+static int launch_common(bool adjoint, int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj,
+                         const dmpc_solver_params* params, void* workspace, size_t workspace_bytes, void* stream) {
+  DevArgs* args = new DevArgs;
+  size_t ws = 0, sm = 0;
+  int thr = 0;
+  int rc = fill_args(n_groups, groups, adj, params, args, &ws, &sm, &thr);
+  if (rc != DMPC_OK) {
+    delete args;
+    return rc;
+  }
+  if (ws > workspace_bytes || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0) {
+    delete args;
+    return DMPC_ERR_WORKSPACE;
+  }
+  if (args->total_blocks == 0) {
+    delete args;
+    return DMPC_OK;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e;
+  if (adjoint) {
+    e = cudaFuncSetAttribute(k_sqp_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) {
+      k_sqp_adj<<<args->total_blocks, thr, sm, st>>>(*args, workspace);
+      e = cudaGetLastError();
+    }
+  } else {
+    e = cudaFuncSetAttribute(k_sqp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) {
+      k_sqp_fwd<<<args->total_blocks, thr, sm, st>>>(*args, workspace);
+      e = cudaGetLastError();
+    }
+  }
+  delete args;
+  return e == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+}
+
+int dmpc_solve_fwd(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  return launch_common(false, n_groups, groups, nullptr, params, workspace, workspace_bytes, stream);
+}
+
+int dmpc_solve_adj(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, const dmpc_solver_params* params,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+  if (!adj) return DMPC_ERR_INVALID;
+  return launch_common(true, n_groups, groups, adj, params, workspace, workspace_bytes, stream);
+}
+
+int dmpc_linearize(const dmpc_group* group, const dmpc_solver_params* params, double* As, double* Bs, double* Cs,
+                   double* Qinv, double* qvec, double* Rinv, double* rvec, void* workspace, size_t workspace_bytes,
+                   void* stream) {
+  if (!group || group->horizons) return DMPC_ERR_INVALID;
+  DevArgs* args = new DevArgs;
+  size_t ws = 0, sm = 0;
+  int thr = 0;
+  int rc = fill_args(1, group, nullptr, params, args, &ws, &sm, &thr);
+  if (rc == DMPC_OK && (ws > workspace_bytes || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0))
+    rc = DMPC_ERR_WORKSPACE;
+  if (rc == DMPC_OK && args->total_blocks > 0) {
+    k_linearize<<<args->total_blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*args, workspace, As, Bs, Cs,
+                                                                                        Qinv, qvec, Rinv, rvec);
+    if (cudaGetLastError() != cudaSuccess) rc = DMPC_ERR_CUDA;
+  }
+  delete args;
+  return rc;
+}
+
+int dmpc_compute_gamma(int batch, int N, int nx, int nu, const double* As_x_Qinv, const double* Asnext_x_Qinvnext,
+                       const double* Bs_x_Rinv, const double* Cs, const double* Q0inv, const double* qvec,
+                       const double* rvec, double* gamma, void* stream) {
+  if (batch < 0 || N < 1 || nx < 1 || nx > DMPC_MAX_NX || nu < 1 || nu > DMPC_MAX_NU) return DMPC_ERR_INVALID;
+  if (batch == 0) return DMPC_OK;
+  k_gamma_dense<<<batch, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(N, nx, nu, As_x_Qinv, Asnext_x_Qinvnext,
+                                                                           Bs_x_Rinv, Cs, Q0inv, qvec, rvec, gamma);
+  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+}
+
+int dmpc_kkt_recover(int batch, int N, int nx, int nu, const double* lambda, const double* As_next, const double* As,
+                     const double* Bs, const double* Qinv, const double* qvec, const double* Rinv, const double* rvec,
+                     double* states, double* controls, void* stream) {
+  if (batch < 0 || N < 1 || nx < 1 || nx > DMPC_MAX_NX || nu < 1 || nu > DMPC_MAX_NU) return DMPC_ERR_INVALID;
+  if (batch == 0) return DMPC_OK;
+  const size_t sm = 2 * (size_t)(N + 1) * nx * sizeof(double);
+  if (sm > 227 * 1024) return DMPC_ERR_UNSUPPORTED;
+  cudaError_t e = cudaFuncSetAttribute(k_recover_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return DMPC_ERR_CUDA;
+  k_recover_dense<<<batch, 256, sm, reinterpret_cast<cudaStream_t>(stream)>>>(N, nx, nu, lambda, As_next, As, Bs,
+                                                                              Qinv, qvec, Rinv, rvec, states, controls);
+  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+}
+
+double dmpc_probe_fp32_fma(int blocks, int iters, float* out, void* stream) {
+  if (blocks < 1 || iters < 1 || !out) return -1.0;
+  k_fma_probe<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(iters, 1.0f, out);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  return (double)blocks * 256.0 * (double)iters * 64.0 * 2.0;  // flops issued
+}
+
+size_t dmpc_schur_workspace_size(int batch, int N, int nx) {
+  return align_up((size_t)batch * 4 * (N + 1) * nx * nx * sizeof(double), 256);
+}
+
+int dmpc_schur_assemble(int batch, int N, int nx, int nu, const double* As_next, const double* As, const double* Bs,
+                        const double* Cs, const double* Qinv, const double* qvec, const double* Rinv,
+                        const double* rvec, double* S, double* Phiinv, double* gamma, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  if (batch < 0 || N < 1 || nx < 1 || nx > DMPC_MAX_NX || nu < 1 || nu > DMPC_MAX_NU) return DMPC_ERR_INVALID;
+  if (workspace_bytes < dmpc_schur_workspace_size(batch, N, nx)) return DMPC_ERR_WORKSPACE;
+  if (batch == 0) return DMPC_OK;
+  k_schur_dense<<<batch, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      N, nx, nu, As_next, As, Bs, Cs, Qinv, qvec, Rinv, rvec, S, Phiinv, gamma, reinterpret_cast<double*>(workspace));
+  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+}
+
+int dmpc_pcg_solve(int batch, int N, int nx, int nu, const double* S, const double* Phiinv, const double* gamma,
+                   const double* lambda_guess, const double* As_next, const double* As, const double* Bs,
+                   const double* Qinv, const double* qvec, const double* Rinv, const double* rvec, int max_iter,
+                   double tol_epsilon, double* lambda, double* states, double* controls, int32_t* num_iterations,
+                   double* convergence_eta, void* stream) {
+  if (batch < 0 || N < 1 || nx < 1 || nx > DMPC_MAX_NX || nu < 1 || nu > DMPC_MAX_NU) return DMPC_ERR_INVALID;
+  if (batch == 0) return DMPC_OK;
+  const size_t sm = 64 * sizeof(double) + 5 * (size_t)(N + 1) * nx * sizeof(double);
+  if (sm > 227 * 1024) return DMPC_ERR_UNSUPPORTED;
+  cudaError_t e = cudaFuncSetAttribute(k_pcg_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return DMPC_ERR_CUDA;
+  k_pcg_dense<<<batch, 256, sm, reinterpret_cast<cudaStream_t>(stream)>>>(
+      N, nx, nu, S, Phiinv, gamma, lambda_guess, As_next, As, Bs, Qinv, qvec, Rinv, rvec, max_iter, tol_epsilon,
+      lambda, states, controls, num_iterations, convergence_eta);
+  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+}
+
+}  // extern "C"

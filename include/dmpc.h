@@ -1,0 +1,241 @@
+/*
+ * dmpc.h -- C ABI of the B200 (sm_100a) batched differentiable-MPC inner solve.
+ *
+ * The library solves many independent optimal-control problems of the form
+ *
+ *   min  sum_{t<N} w_x.(x_t - xref_t)^2 + w_u.(u_t - uref_t)^2
+ *        + (w_x + w_f).(x_N - x_final)^2
+ *   s.t. x_0 = x_init,  x_{t+1} = F(x_t, u_t)   (one Euler / midpoint / RK4 step)
+ *
+ * by SQP whose QPs are solved with the Schur-complement block-tridiagonal
+ * preconditioned conjugate gradient method, and differentiates the solution
+ * with the implicit-function adjoint that reuses the same Schur/PCG machinery.
+ * It replaces, call for call, the reference's JAX solver:
+ *
+ *   dmpc_solve_fwd      <- SQPSolver._solve                 diffmpc/solvers/sqp.py:436-560
+ *   dmpc_solve_adj      <- SQPSolver _solve_bwd/_solve_bwd_pcg/_compute_mixed_derivatives
+ *                                                            diffmpc/solvers/sqp.py:605-798
+ *   dmpc_schur_assemble <- PCGOptimalControl.compute_S_Phiinv + compute_gamma
+ *                                                            diffmpc/solvers/pcg.py:160-288
+ *   dmpc_pcg_solve      <- PCGOptimalControl.solve_KKT_Schur diffmpc/solvers/pcg.py:350-445
+ *                          (+ get_states_controls_from_kkt_multipliers pcg.py:290-348)
+ *   dmpc_compute_gamma  <- PCGOptimalControl.compute_gamma   diffmpc/solvers/pcg.py:245-288
+ *   dmpc_kkt_recover    <- PCGOptimalControl.get_states_controls_from_kkt_multipliers
+ *                                                            diffmpc/solvers/pcg.py:290-348
+ *   dmpc_linearize      <- OptimalControlProblem.get_dynamics_linearized_matrices_with_states_controls
+ *                          + get_cost_linearized_matrices + SQPSolver.get_cost_terms
+ *                                                            diffmpc/problems/optimal_control_problem.py:249-398,
+ *                                                            diffmpc/solvers/sqp.py:160-260
+ *
+ * Conventions.  Every pointer is a DEVICE pointer unless stated otherwise;
+ * floating-point data is float64, row-major, instance-major (SoA over the
+ * batch).  N is the reference's `horizon`; K = N + 1 knots.  All calls are
+ * stream-ordered, never synchronise the host, and never allocate: scratch
+ * memory is the caller's `workspace` (size from dmpc_workspace_size).
+ * Return value: DMPC_OK or a DMPC_ERR_* code; per-instance solver status is
+ * written to device memory with the reference's values (0 success, -100 error).
+ */
+#ifndef DMPC_H_
+#define DMPC_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DMPC_ABI_VERSION 1
+
+/* return codes */
+#define DMPC_OK 0
+#define DMPC_ERR_INVALID 1      /* bad descriptor / sizes (the reference raises ValueError/KeyError) */
+#define DMPC_ERR_WORKSPACE 2    /* workspace too small or misaligned */
+#define DMPC_ERR_CUDA 3         /* a CUDA runtime call failed */
+#define DMPC_ERR_UNSUPPORTED 4  /* model or option not supported (reference: NotImplementedError) */
+
+/* per-instance solver status, SolverReturnStatus (diffmpc/solvers/sqp.py:31-35) */
+#define DMPC_STATUS_SUCCESS 0
+#define DMPC_STATUS_ERROR (-100)
+
+/* dynamics models (diffmpc/dynamics/*.py).  Model parameter vectors:
+ *   LINEAR      nx, nu free;  [A (nx*nx), B (nx*nu), b (nx)]     linear_dynamics.py:46-70
+ *   QUADROTOR   nx=13, nu=4;  [mass, inertia (3x3 row-major, 9)] quadrotor_dynamics.py:84-133
+ *   SPACECRAFT  nx=3,  nu=3;  [inertia_vector (3)]                spacecraft_dynamics.py:31-66
+ *   ATTITUDE    nx=7,  nu=3;  [inertia_vector (3)]  quaternion + rate (no reference counterpart)
+ *   CARTPOLE    nx=4,  nu=1;  [masscart, masspole, length, gravity] cartpole_dynamics.py:36-80 */
+#define DMPC_MODEL_LINEAR 0
+#define DMPC_MODEL_QUADROTOR 1
+#define DMPC_MODEL_SPACECRAFT 2
+#define DMPC_MODEL_ATTITUDE 3
+#define DMPC_MODEL_CARTPOLE 4
+
+/* DiscretizationScheme (diffmpc/dynamics/integrators.py:12-17) */
+#define DMPC_EULER 0
+#define DMPC_MIDPOINT 1
+#define DMPC_RK4 2
+
+/* PCG arithmetic */
+#define DMPC_PREC_FP64 0   /* all-FP64 PCG, the reference's arithmetic */
+#define DMPC_PREC_MIXED 1  /* FP32 PCG iterations + FP64 iterative refinement */
+
+#define DMPC_MAX_NX 32
+#define DMPC_MAX_NU 16
+#define DMPC_MAX_ALPHAS 8
+#define DMPC_MAX_PARAM_GRADS 64
+#define DMPC_MAX_GROUPS 8
+
+/* Solver options: diffmpc/solvers/params/sqp.yaml plus the precision controls. */
+typedef struct dmpc_solver_params {
+  double tol_convergence;         /* sqp.yaml tol_convergence */
+  int32_t num_scp_iteration_max;  /* sqp.yaml num_scp_iteration_max */
+  int32_t linesearch;             /* sqp.yaml linesearch (0/1) */
+  double linesearch_eta;          /* sqp.yaml linesearch_eta */
+  int32_t n_alphas;               /* len(linesearch_alphas) <= DMPC_MAX_ALPHAS */
+  double alphas[DMPC_MAX_ALPHAS]; /* sqp.yaml linesearch_alphas */
+  int32_t warm_start_backward;    /* sqp.yaml warm_start_backward */
+  int32_t pcg_max_iter;           /* sqp.yaml pcg.max_iter */
+  double pcg_tol_epsilon;         /* sqp.yaml pcg.tol_epsilon (absolute, on eta = r^T Phi^-1 r) */
+  int32_t precision;              /* DMPC_PREC_* */
+  int32_t max_refinement;         /* MIXED: outer FP64 refinement steps per QP solve */
+  double inner_rel_tol;           /* MIXED: inner FP32 PCG stops when eta32 <= inner_rel_tol * eta at restart */
+  int32_t threads_per_block;      /* 0 = automatic (autotuned table) */
+  int32_t blocks_in_smem;         /* -1 auto, 0 force global-memory blocks, 1 require shared memory */
+} dmpc_solver_params;
+
+/* One group = instances sharing model, nx, nu and max horizon (a batch).
+ * Per-instance horizons may differ (ragged batch): arrays are padded to K = horizon + 1
+ * rows and instance i uses its first horizons[i] + 1 rows. */
+typedef struct dmpc_group {
+  int32_t model, nx, nu;
+  int32_t horizon;                 /* N (maximum over the group when `horizons` is given) */
+  int32_t batch;                   /* number of instances */
+  int32_t scheme;                  /* DMPC_EULER / DMPC_MIDPOINT / DMPC_RK4 */
+  int32_t penalize_control_reference;
+  int32_t n_model_params;          /* length of each instance's model parameter vector */
+  const int32_t* horizons;         /* (batch) per-instance N_i in [1, horizon], or NULL */
+  /* problem parameters (optimal_control_problem.py:153-206 key names) */
+  const double* dt;                /* (batch) discretization_resolution */
+  const double* initial_state;     /* (batch, nx) */
+  const double* final_state;       /* (batch, nx) */
+  const double* reference_state;   /* (batch, K, nx) reference_state_trajectory */
+  const double* reference_control; /* (batch, K, nu) reference_control_trajectory */
+  const double* w_x;               /* (batch, nx) weights_penalization_reference_state_trajectory */
+  const double* w_u;               /* (batch, nu) weights_penalization_control_squared */
+  const double* w_f;               /* (batch, nx) weights_penalization_final_state */
+  const double* model_params;      /* (batch, n_model_params) */
+  /* initial guess on entry, solution on exit (SQPSolution fields, sqp.py:38-57) */
+  double* states;                  /* (batch, K, nx) */
+  double* controls;                /* (batch, K, nu); row N is zero on exit (pcg.py:346) */
+  double* dual;                    /* (batch, K, nx) KKT multipliers */
+  double* convergence_error;       /* (batch) in: guess value, out: final */
+  int32_t* status;                 /* (batch) out */
+  int32_t* num_iter;               /* (batch) out */
+  double* convergence_errors;      /* (batch, num_scp_iteration_max) in/out */
+  double* linesearch_alphas;       /* (batch, num_scp_iteration_max) in/out */
+  int32_t* num_pcg_iters;          /* (batch, num_scp_iteration_max) in/out */
+  double* lin_states;              /* (batch, K, nx) out: iterate of the last linearization */
+  double* lin_controls;            /* (batch, K, nu) out */
+} dmpc_group;
+
+/* Adjoint inputs/outputs for one group (sqp.py:668-798).  Gradient outputs
+ * that are NULL are not computed. */
+typedef struct dmpc_adjoint {
+  const double* dl_dstates;          /* (batch, K, nx) cotangent of states */
+  const double* dl_dcontrols;        /* (batch, K, nu) cotangent of controls (row N unused) */
+  const double* dual_backward_guess; /* (batch, K, nx) warm start, or NULL for zeros */
+  double* dual_backward;             /* (batch, K, nx) out: adjoint multipliers */
+  int32_t* num_pcg_iter;             /* (batch) out, may be NULL */
+  double* g_initial_state;           /* (batch, nx) */
+  double* g_final_state;             /* (batch, nx) */
+  double* g_w_x;                     /* (batch, nx) */
+  double* g_w_u;                     /* (batch, nu) */
+  double* g_w_f;                     /* (batch, nx) */
+  double* g_reference_state;         /* (batch, K, nx) */
+  double* g_reference_control;       /* (batch, K, nu) */
+  int32_t n_param_grads;             /* number of model-parameter gradients (<= DMPC_MAX_PARAM_GRADS) */
+  const int32_t* param_grad_index;   /* (n_param_grads) HOST array of model-parameter indices */
+  double* g_model_params;            /* (batch, n_param_grads) */
+  /* adjoint solution (x~, u~), optional (batch, K, nx) / (batch, K, nu) */
+  double* adj_states;
+  double* adj_controls;
+} dmpc_adjoint;
+
+int dmpc_abi_version(void);
+const char* dmpc_error_string(int code);
+
+/* Bytes of workspace the forward/adjoint calls need for these groups. */
+size_t dmpc_workspace_size(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params);
+
+/* Fills `params` with the reference defaults (sqp.yaml:1-11) and MIXED precision. */
+void dmpc_default_params(dmpc_solver_params* params);
+
+/* Forward SQP solve of every instance of every group (n_groups <= DMPC_MAX_GROUPS) in ONE kernel launch
+ * (SQPSolver._solve, sqp.py:436-560).  Workspace must be 256-byte aligned. */
+int dmpc_solve_fwd(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint solve + gradients at the forward solution held in `groups`
+ * (states/controls/dual = z*, lambda*; lin_states/lin_controls = last linearization).
+ * One launch for all groups (sqp.py:668-798). */
+int dmpc_solve_adj(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj,
+                   const dmpc_solver_params* params, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/* ---- lower-level entry points, reference dense layouts (pcg.py:13-67) ---- */
+
+/* Linearize at (states, controls) of `group` (no solve): writes As (batch,N,nx,nx),
+ * Bs (batch,N,nx,nu), Cs (batch,K,nx), Qinv (batch,K,nx,nx), qvec (batch,K,nx),
+ * Rinv (batch,N,nu,nu), rvec (batch,N,nu).  As_next is -I (optimal_control_problem.py:393-397).
+ * Uniform horizon only; workspace from dmpc_workspace_size(1, group, params). */
+int dmpc_linearize(const dmpc_group* group, const dmpc_solver_params* params, double* As, double* Bs,
+                   double* Cs, double* Qinv, double* qvec, double* Rinv, double* rvec, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/* compute_S_Phiinv + compute_gamma for general QP data (pcg.py:160-288), batch of
+ * `batch` uniform problems: As_next, As (batch,N,nx,nx), Bs (batch,N,nx,nu), Cs (batch,K,nx),
+ * Qinv (batch,K,nx,nx), qvec (batch,K,nx), Rinv (batch,N,nu,nu), rvec (batch,N,nu)
+ *  -> S, Phiinv (batch,K,nx,3nx), gamma (batch,K,nx). */
+int dmpc_schur_assemble(int batch, int N, int nx, int nu, const double* As_next, const double* As,
+                        const double* Bs, const double* Cs, const double* Qinv, const double* qvec,
+                        const double* Rinv, const double* rvec, double* S, double* Phiinv,
+                        double* gamma, void* workspace, size_t workspace_bytes, void* stream);
+size_t dmpc_schur_workspace_size(int batch, int N, int nx);
+
+/* solve_KKT_Schur on the dense S / Phiinv layout (pcg.py:350-445), FP64, with the
+ * reference's stopping rule; then (x, u) from lambda (pcg.py:290-348).
+ * lambda_guess (batch,K,nx) -> lambda, states (batch,K,nx), controls (batch,K,nu),
+ * num_iterations (batch), convergence_eta (batch). */
+int dmpc_pcg_solve(int batch, int N, int nx, int nu, const double* S, const double* Phiinv,
+                   const double* gamma, const double* lambda_guess, const double* As_next,
+                   const double* As, const double* Bs, const double* Qinv, const double* qvec,
+                   const double* Rinv, const double* rvec, int max_iter, double tol_epsilon,
+                   double* lambda, double* states, double* controls, int32_t* num_iterations,
+                   double* convergence_eta, void* stream);
+
+/* compute_gamma from premultiplied matrices (pcg.py:245-288): As_x_Qinv, Asnext_x_Qinvnext
+ * (batch,N,nx,nx), Bs_x_Rinv (batch,N,nx,nu), Cs (batch,K,nx), Q0inv (batch,nx,nx),
+ * qvec (batch,K,nx), rvec (batch,N,nu) -> gamma (batch,K,nx). */
+int dmpc_compute_gamma(int batch, int N, int nx, int nu, const double* As_x_Qinv,
+                       const double* Asnext_x_Qinvnext, const double* Bs_x_Rinv, const double* Cs,
+                       const double* Q0inv, const double* qvec, const double* rvec, double* gamma,
+                       void* stream);
+
+/* get_states_controls_from_kkt_multipliers (pcg.py:290-348), general dense matrices:
+ * lambda (batch,K,nx) -> states (batch,K,nx), controls (batch,K,nu) with row N zero. */
+int dmpc_kkt_recover(int batch, int N, int nx, int nu, const double* lambda, const double* As_next,
+                     const double* As, const double* Bs, const double* Qinv, const double* qvec,
+                     const double* Rinv, const double* rvec, double* states, double* controls,
+                     void* stream);
+
+/* Diagnostic: launches an FP32 FMA throughput probe (`blocks` x 256 threads, `iters`
+ * rounds of 64 FMAs per thread) on `stream` and returns the FLOPs it issues, or -1.
+ * Timing it with events gives the measured FP32 CUDA-core peak used as the roofline
+ * denominator of the shared-memory-resident PCG.  `out` (device, >= blocks floats) is
+ * written only to keep the computation live.  No reference counterpart. */
+double dmpc_probe_fp32_fma(int blocks, int iters, float* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DMPC_H_ */

@@ -1,0 +1,96 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol
+declared in include/dmpc.h, its structs match ctypes, and host-side
+validation rejects bad descriptors without launching anything."""
+
+import ctypes
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+from diffmpc_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "dmpc.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|void|double|const char\*)\s+(dmpc_\w+)\(", text, re.M)))
+
+
+def test_library_loads_and_exports_every_header_symbol():
+    lib = _lib.load()
+    names = header_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.EXPORTED_SYMBOLS)
+    assert lib.dmpc_abi_version() == 1
+
+
+def test_defaults_match_reference_yaml():
+    p = _lib.SolverParams()
+    _lib.load().dmpc_default_params(p)
+    assert p.tol_convergence == 1e-8 and p.num_scp_iteration_max == 15
+    assert p.linesearch == 0 and p.linesearch_eta == 0.4
+    assert list(p.alphas)[: p.n_alphas] == [0.01, 0.1, 0.3, 0.7, 1.0]
+    assert p.warm_start_backward == 1 and p.pcg_max_iter == 10000 and p.pcg_tol_epsilon == 1e-9
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc missing")
+def test_struct_layout_matches_c(tmp_path):
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "%s"\n'
+        "int main(){printf(\"%%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n\","
+        "sizeof(dmpc_solver_params),sizeof(dmpc_group),sizeof(dmpc_adjoint),"
+        "offsetof(dmpc_solver_params,blocks_in_smem),offsetof(dmpc_group,lin_controls),"
+        "offsetof(dmpc_adjoint,param_grad_index),offsetof(dmpc_adjoint,adj_controls));}\n" % HEADER
+    )
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [
+        ctypes.sizeof(_lib.SolverParams), ctypes.sizeof(_lib.Group), ctypes.sizeof(_lib.Adjoint),
+        _lib.SolverParams.blocks_in_smem.offset, _lib.Group.lin_controls.offset,
+        _lib.Adjoint.param_grad_index.offset, _lib.Adjoint.adj_controls.offset,
+    ]
+    assert got == want
+
+
+def _group(model=1, nx=13, nu=4, N=10, batch=2, P=10):
+    g = _lib.Group()
+    g.model, g.nx, g.nu, g.horizon, g.batch, g.scheme, g.n_model_params = model, nx, nu, N, batch, 2, P
+    return g
+
+
+def test_host_validation_rejects_bad_descriptors():
+    lib = _lib.load()
+    p = _lib.SolverParams()
+    lib.dmpc_default_params(p)
+    assert lib.dmpc_workspace_size(1, _group(), p) > 0
+    assert lib.dmpc_workspace_size(1, _group(nx=12), p) == 0          # quadrotor needs nx = 13
+    assert lib.dmpc_workspace_size(1, _group(P=9), p) == 0            # wrong parameter count
+    assert lib.dmpc_workspace_size(1, _group(model=9), p) == 0        # unknown model
+    assert lib.dmpc_workspace_size(0, _group(), p) == 0               # no groups
+    g = _group(nx=12)
+    assert lib.dmpc_solve_fwd(1, g, p, None, 0, None) == 4            # DMPC_ERR_UNSUPPORTED
+    assert lib.dmpc_solve_fwd(1, _group(), p, None, 0, None) == 2     # DMPC_ERR_WORKSPACE
+    bad = _lib.SolverParams()
+    lib.dmpc_default_params(bad)
+    bad.n_alphas = 0
+    assert lib.dmpc_solve_fwd(1, _group(), bad, None, 0, None) == 1   # DMPC_ERR_INVALID
+    assert lib.dmpc_error_string(2) == b"workspace too small or misaligned"
+
+
+def test_workspace_grows_with_batch_and_horizon():
+    lib = _lib.load()
+    p = _lib.SolverParams()
+    lib.dmpc_default_params(p)
+    a = lib.dmpc_workspace_size(1, _group(batch=1), p)
+    b = lib.dmpc_workspace_size(1, _group(batch=4), p)
+    c = lib.dmpc_workspace_size(1, _group(batch=1, N=20), p)
+    assert b == 4 * a and c > a and a % 256 == 0
