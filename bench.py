@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Benchmark: batched forward + adjoint MPC solves/s, quadrotor N=60 (K=61 knots), B=4096.
+
+One step = one batched SQP forward solve (``k_sqp_fwd``: linearize -> Schur
+assembly -> PCG -> recover, up to 15 SQP iterations) of 4096 quadrotor MPC
+instances plus the hand-written adjoint (``k_sqp_adj``) of the loss
+``sum_i ||u_0^i||^2`` with respect to x0, the diag(Q)/diag(R) log-weights and
+the mass.  Synthetic, seeded inputs (``diffmpc_b200.workloads.quadrotor``).
+
+Contract: ``python bench.py --gpus N --steps K --warmup W`` prints ONE JSON line
+on rank 0.  N > 1 runs under torchrun, one process per GPU, each rank solving
+its own batch of 4096 (weak scaling, no data-path collective: instances are
+independent).  ``--impl reference`` times the reference algorithm's CPU
+implementation (the float64 oracle restatement; the JAX reference cannot be
+installed offline) on the host cores.
+"""
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd MPC solves/s, quadrotor T=60 B=4096, vs plain FP64 GPU @1e-6 rel"
+UNIT = "solves/s"
+GRAD_KEYS = ("initial_state", "weights_penalization_reference_state_trajectory",
+             "weights_penalization_control_squared", "mass")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--horizon", type=int, default=60)
+    ap.add_argument("--pcg-tol", type=float, default=1e-11)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU-baseline sample")
+    ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")
+    ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def max_over_ranks(value, device=None):
+    """Max of a float over all ranks (identity when not distributed)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(device=None):
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        if device is not None and device.type == "cuda":
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons every 200 ms while active."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+def build(args, rank):
+    from diffmpc_b200 import workloads
+
+    dyn, st, bt, sp = workloads.quadrotor(B=args.batch, N=args.horizon, seed=1002 + rank)
+    sp["precision"] = args.precision
+    sp["pcg"]["tol_epsilon"] = args.pcg_tol
+    return dyn, st, bt, sp
+
+
+def algorithmic_flops(nx, nu, N, sqp_iters, pcg_iters, adj_pcg_iters, rk4=True):
+    """Algorithmic FLOPs of the reference's dense algorithm for the executed iteration
+    counts: F_pcg = 12 K nx^2 + 10 K nx per PCG iteration, F_setup = K (16 nx^3 + 4 nx^2 nu)
+    per QP assembly, F_lin = N (nx + nu) s F_f per linearization (s = 4 for RK4, F_f = 130
+    flops for the quadrotor state_dot)."""
+    K = N + 1
+    f_pcg = 12 * K * nx * nx + 10 * K * nx
+    f_setup = K * (16 * nx**3 + 4 * nx * nx * nu)
+    f_lin = N * (nx + nu) * (4 if rk4 else 1) * 130
+    fwd = sqp_iters * (f_setup + f_lin) + pcg_iters * f_pcg
+    adj = (f_setup + f_lin) + adj_pcg_iters * f_pcg
+    return fwd, adj, f_pcg
+
+
+def fp32_peak_tflops(torch, lib):
+    """Measured FP32 FMA throughput of this GPU (libdmpc's probe kernel, CUDA events)."""
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    blocks = props.multi_processor_count * 8
+    out = torch.zeros(blocks, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    lib.dmpc_probe_fp32_fma(blocks, 256, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        flops = lib.dmpc_probe_fp32_fma(blocks, 4096, out.data_ptr(), stream)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, flops / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from diffmpc_b200 import OptimalControlProblem, SQPSolver, _lib, workloads
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    lib = _lib.load()
+    dyn, st, bt, sp = build(args, rank)
+    B, N, nx, nu = args.batch, args.horizon, dyn.num_states, dyn.num_controls
+    solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp, device=device)
+    p = workloads.to_device(bt, device)
+    l2_flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def one_step(params):
+        lw_x = torch.log(params["weights_penalization_reference_state_trajectory"]).detach().requires_grad_(True)
+        lw_u = torch.log(params["weights_penalization_control_squared"]).detach().requires_grad_(True)
+        x0 = params["initial_state"].detach().clone().requires_grad_(True)
+        mass = params["mass"].detach().clone().requires_grad_(True)
+        weights = {
+            "initial_state": x0,
+            "weights_penalization_reference_state_trajectory": torch.exp(lw_x),
+            "weights_penalization_control_squared": torch.exp(lw_u),
+            "mass": mass,
+        }
+        guess = solver.initial_guess(params)
+        sol = solver.solve(guess, params, weights)
+        loss = (sol.controls[:, 0] ** 2).sum()
+        loss.backward()
+        return sol, {"initial_state": x0.grad, "log_w_x": lw_x.grad, "log_w_u": lw_u.grad, "mass": mass.grad}
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        sol, grads = one_step(p)
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs, kernel events on the launching stream
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    step_ms, fwd_ms, adj_ms = [], [], []
+    barrier(device)
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        l2_flush.zero_()  # > L2 (126 MB): every step starts cold
+        solver.kernel_events = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sol, grads = one_step(p)
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        for name, a, b in solver.kernel_events:
+            (fwd_ms if name == "k_sqp_fwd" else adj_ms).append(a.elapsed_time(b))
+    barrier(device)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    solver.kernel_events = None
+    total_ms = max_over_ranks(sum(step_ms), device)
+    ms_per_step = total_ms / args.steps
+    value = world * B * args.steps / (total_ms * 1e-3)
+    gpu_launches = args.steps * 2
+
+    # ---- roofline of the dominant kernel (k_sqp_fwd)
+    sqp_iters = float(sol.num_iter.double().sum())
+    pcg_iters = float(sol.num_pcg_iters.double().sum())
+    adj_iters = float(solver.last_adjoint_pcg_iters.double().sum()) if solver.last_adjoint_pcg_iters is not None else 0.0
+    f_fwd, f_adj, f_pcg = algorithmic_flops(nx, nu, N, sqp_iters, pcg_iters, adj_iters)
+    fwd_avg = statistics.mean(fwd_ms)
+    peak = fp32_peak_tflops(torch, lib)
+    achieved = f_fwd / (fwd_avg * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "k_sqp_fwd_traffic.json")
+    if os.path.exists(prof):
+        try:
+            t = json.load(open(prof))
+            traffic = t["dram_bytes_per_instance"] * B
+        except (ValueError, KeyError):
+            traffic = None
+    roofline = {
+        "bound": "fp32", "kernel": "k_sqp_fwd", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+        "peak_source": "measured: libdmpc FP32 FMA probe on this GPU (MEASURED_PEAKS.json has no FP32 figure)",
+        "algorithmic_flops_per_launch": f_fwd, "kernel_ms": fwd_avg,
+        "adj_kernel_ms": statistics.mean(adj_ms) if adj_ms else None,
+        "pcg_iters_per_instance": pcg_iters / B, "sqp_iters_per_instance": sqp_iters / B,
+        "adj_pcg_iters_per_instance": adj_iters / B,
+        "adj_achieved_tflops": (f_adj * B / (statistics.mean(adj_ms) * 1e-3) / 1e12) if adj_ms else None,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {
+            "workload": "quadrotor N=60 (K=61), RK4 dt=0.05, fwd SQP (<=15 it, tol 1e-8) + adjoint, loss sum u0^2",
+            "batch_per_gpu": B, "horizon": N, "nx": nx, "nu": nu, "pcg_tol_epsilon": args.pcg_tol,
+            "precision": args.precision, "parallelism": f"replicas x{world}",
+            "l2": "512 MB buffer written between timed steps; workspace 2.7 GB > L2",
+        },
+        "roofline": roofline, "clocks": clocks, "gpu_launches": gpu_launches,
+    }
+
+    if not args.no_extras:
+        # ---- e2e through the public API with host buffers (pinned), copies inside the region
+        host = {k: (v.pin_memory() if isinstance(v, torch.Tensor) else v) for k, v in bt.items()}
+        h2d = sum(v.numel() * v.element_size() for v in host.values() if isinstance(v, torch.Tensor))
+        out_host = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in grads.items()}
+        u0_host = torch.empty((B, nu), dtype=torch.float64, pin_memory=True)
+        d2h = sum(v.numel() * v.element_size() for v in out_host.values()) + u0_host.numel() * 8
+        e2e_ms = []
+        for it in range(args.warmup + args.steps):
+            l2_flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pd = {k: (v.to(device, non_blocking=True) if isinstance(v, torch.Tensor) else v) for k, v in host.items()}
+            s2, g2 = one_step(pd)
+            for k in out_host:
+                out_host[k].copy_(g2[k], non_blocking=True)
+            u0_host.copy_(s2.controls[:, 0], non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            if it >= args.warmup:
+                e2e_ms.append(e0.elapsed_time(e1))
+        e2e_total = max_over_ranks(sum(e2e_ms), device)
+        line["e2e"] = {"value": world * B * args.steps / (e2e_total * 1e-3), "unit": UNIT,
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    if rank == 0 and not args.no_extras:
+        # ---- plain all-FP64 one-instance-per-launch GPU path (the metric's denominator)
+        sp64 = dict(sp)
+        sp64["precision"] = "fp64"
+        solver64 = SQPSolver(OptimalControlProblem(dyn, st), params=sp64, device=device)
+        S = min(args.fp64_sample, B)
+
+        def one64(i):
+            pi = workloads.subset(p, slice(i, i + 1))
+            lw = torch.log(pi["weights_penalization_reference_state_trajectory"]).requires_grad_(True)
+            w = {"weights_penalization_reference_state_trajectory": torch.exp(lw),
+                 "initial_state": pi["initial_state"].clone().requires_grad_(True),
+                 "weights_penalization_control_squared": pi["weights_penalization_control_squared"].clone().requires_grad_(True),
+                 "mass": pi["mass"].clone().requires_grad_(True)}
+            s = solver64.solve(solver64.initial_guess(pi), pi, w)
+            (s.controls[:, 0] ** 2).sum().backward()
+            return s
+
+        one64(0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sols64 = [one64(i) for i in range(S)]
+        e1.record()
+        torch.cuda.synchronize()
+        fp64_rate = S / (e0.elapsed_time(e1) * 1e-3)
+        ctrl64 = torch.cat([s.controls for s in sols64]).cpu()
+        rel64 = float((sol.controls[:S].detach().cpu() - ctrl64).abs().max() / ctrl64.abs().max())
+        line["fp64_one_per_launch"] = {
+            "value": fp64_rate, "unit": UNIT, "sample": f"{S} instances, one fwd+adj launch pair each",
+            "speedup_of_value": value / (world * fp64_rate) if fp64_rate > 0 else None,
+            "max_rel_control_diff_mixed_vs_fp64": rel64,
+        }
+        # ---- CPU baseline: float64 oracle on a bounded sample, all host cores
+        line["cpu_baseline"] = cpu_baseline(args, sol, grads, bt, dyn, st, sp)
+
+    if world > 1:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _oracle_run(dyn, st, bt, sp, idx):
+    """fwd + adjoint of the oracle on instances `idx`; returns (controls, grads, seconds)."""
+    import torch
+
+    from diffmpc_b200 import workloads
+    from oracle.models import make_model
+    from oracle.ocp import STATIC_KEYS, OptimalControlProblem
+    from oracle.sqp import SQPSolver as OracleSolver
+
+    sub = workloads.subset(bt, idx)
+    w = {k: sub[k] for k in GRAD_KEYS}
+    t0 = time.perf_counter()
+    s = OracleSolver(OptimalControlProblem(make_model(dyn.model_name, dyn.num_states, dyn.num_controls), st), params=sp)
+    sol = s._solve(s.initial_guess({k: v for k, v in sub.items() if k not in STATIC_KEYS}), sub, w)
+    dlu = torch.zeros_like(sol.controls)
+    dlu[:, 0] = 2 * sol.controls[:, 0]
+    g, _, _ = s.solve_bwd(sol, w, sub, torch.zeros_like(sol.states), dlu, torch.zeros_like(sol.dual))
+    dt = time.perf_counter() - t0
+    return sol.controls, g, dt
+
+
+def cpu_baseline(args, sol, grads, bt, dyn, st, sp):
+    import torch
+
+    n = os.cpu_count() or 1
+    torch.set_num_threads(n)
+    S = min(args.cpu_sample, args.batch)
+    _oracle_run(dyn, st, bt, sp, slice(0, 1))  # warm-up
+    ctrl, g, secs = _oracle_run(dyn, st, bt, sp, slice(0, S))
+    gpu_ctrl = sol.controls[:S].detach().cpu()
+    rel_c = float((gpu_ctrl - ctrl).abs().amax(dim=(1, 2)).max() / ctrl.abs().max())
+    gw = grads["log_w_x"][:S].cpu()
+    ow = g["weights_penalization_reference_state_trajectory"] * bt["weights_penalization_reference_state_trajectory"][:S]
+    rel_g = float((gw - ow).abs().max() / ow.abs().max())
+    gm = grads["mass"][:S].cpu()
+    rel_m = float((gm - g["mass"]).abs().max() / g["mass"].abs().max())
+    return {
+        "value": S / secs, "unit": UNIT, "cores": n, "kind": "port",
+        "sample": f"{S} of the {args.batch} instances, fwd+adjoint, float64 oracle (torch CPU), one run after warm-up",
+        "max_rel_control_err_vs_oracle": rel_c, "max_rel_grad_err_vs_oracle": max(rel_g, rel_m),
+    }
+
+
+def run_reference(args):
+    """Reference arm: the reference algorithm on the host CPU (float64 oracle restatement)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import torch
+
+    n = os.cpu_count() or 1
+    torch.set_num_threads(n)
+    dyn, st, bt, sp = build(args, 0)
+    S = max(1, min(args.cpu_sample, args.batch))
+    times = []
+    for it in range(args.warmup + args.steps):
+        lo = (it * S) % args.batch
+        _, _, secs = _oracle_run(dyn, st, bt, sp, slice(lo, lo + S))
+        if it >= args.warmup:
+            times.append(secs)
+    value = S * len(times) / sum(times)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "quadrotor N=60 (K=61), RK4 dt=0.05, fwd SQP (<=15 it, tol 1e-8) + adjoint, loss sum u0^2",
+                   "batch_per_gpu": args.batch, "horizon": args.horizon, "pcg_tol_epsilon": args.pcg_tol,
+                   "sample_per_step": S},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": n, "kind": "port",
+                         "sample": f"{S} instances per step (fwd+adjoint), float64 oracle restatement of the "
+                                   "reference JAX solver (JAX is not installable offline)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

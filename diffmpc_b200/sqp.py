@@ -232,6 +232,8 @@ class SQPSolver:
         self._ws = None
         # optional list collecting (name, start_event, end_event) around each kernel launch
         self.kernel_events = None
+        # adjoint PCG iteration counts of the most recent backward pass, (B,) int32
+        self.last_adjoint_pcg_iters = None
         self.solve = self._solve_differentiable
 
     # -- properties (sqp.py:100-133) ------------------------------------------
@@ -339,7 +341,9 @@ class SQPSolver:
         dlu = (g_controls if g_controls is not None else z(B, K, nu)).to(torch.float64).contiguous()
         dbg = None if g_dbg is None else g_dbg.to(torch.float64).contiguous()
         out = {"__dual_backward__": z(B, K, nx)}
+        adj_iters = torch.zeros(B, dtype=torch.int32, device=dev)
         adj = _lib.Adjoint()
+        adj.num_pcg_iter = adj_iters.data_ptr()
         adj.dl_dstates, adj.dl_dcontrols = dlx.data_ptr(), dlu.data_ptr()
         adj.dual_backward_guess = _ptr(dbg)
         adj.dual_backward = out["__dual_backward__"].data_ptr()
@@ -382,6 +386,7 @@ class SQPSolver:
             self._event_end(ev, "k_sqp_adj")
             for j, k in enumerate(chunk):
                 gmp[k] = gbuf[:, j]
+        self.last_adjoint_pcg_iters = adj_iters
         out.update(bufs)
         for k in keys:
             if k in slices:
