@@ -17,6 +17,7 @@ DMPC_MAX_NU = 16
 DMPC_MAX_ALPHAS = 8
 DMPC_MAX_PARAM_GRADS = 64
 DMPC_MAX_GROUPS = 8
+DMPC_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 MODEL_IDS = {"linear": 0, "quadrotor": 1, "spacecraft": 2, "attitude": 3, "cartpole": 4}
 PREC_FP64, PREC_MIXED = 0, 1
@@ -35,6 +36,7 @@ EXPORTED_SYMBOLS = (
     "dmpc_compute_gamma",
     "dmpc_kkt_recover",
     "dmpc_probe_fp32_fma",
+    "dmpc_solve_fwd_noalloc",
 )
 
 _p = ctypes.c_void_p
@@ -167,6 +169,8 @@ def load():
     lib.dmpc_kkt_recover.argtypes = [ctypes.c_int] * 4 + [_p] * 10 + [_p]
     lib.dmpc_probe_fp32_fma.restype = ctypes.c_double
     lib.dmpc_probe_fp32_fma.argtypes = [ctypes.c_int, ctypes.c_int, _p, _p]
+    lib.dmpc_solve_fwd_noalloc.restype = ctypes.c_int
+    lib.dmpc_solve_fwd_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(Group), ctypes.POINTER(SolverParams), _p]
     if lib.dmpc_abi_version() != 1:
         raise DmpcError("libdmpc.so ABI version mismatch")
     _lib = lib

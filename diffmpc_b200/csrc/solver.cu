@@ -26,6 +26,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "../../include/dmpc.h"
 #include "common.cuh"
 #include "dual.cuh"
@@ -1428,6 +1430,19 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
 
 }  // namespace
 
+// Fixed scratch for dmpc_solve_fwd_noalloc.  It is part of this library's device
+// module, so every GPU that loads the library holds these bytes until the process
+// exits.  Host code must not pass `g_noalloc_scratch` itself to a kernel: on the host
+// the name stands for a host-side shadow, not a device address.  The device address
+// is looked up once per device with cudaGetSymbolAddress and cached below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[DMPC_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_device_ptr[kNoallocMaxDevices] = {};
+}  // namespace
+
 extern "C" {
 
 int dmpc_abi_version(void) { return DMPC_ABI_VERSION; }
@@ -1517,6 +1532,35 @@ int dmpc_solve_adj(int n_groups, const dmpc_group* groups, const dmpc_adjoint* a
                    void* workspace, size_t workspace_bytes, void* stream) {
   if (!adj) return DMPC_ERR_INVALID;
   return launch_common(true, n_groups, groups, adj, params, workspace, workspace_bytes, stream);
+}
+
+// Forward solve for callers that cannot allocate device memory: it uses the fixed
+// library-owned scratch array above instead of a caller workspace.  The first call on
+// a device looks up that array's device address (with that device current) and
+// caches it; make that first call outside any stream capture.
+int dmpc_solve_fwd_noalloc(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params, void* stream) {
+  DevArgs* args = new DevArgs;
+  size_t need = 0, sm = 0;
+  int thr = 0;
+  int rc = fill_args(n_groups, groups, nullptr, params, args, &need, &sm, &thr);
+  delete args;
+  if (rc != DMPC_OK) return rc;
+  if (need > (size_t)DMPC_NOALLOC_SCRATCH_BYTES) return DMPC_ERR_WORKSPACE;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DMPC_ERR_CUDA;
+  if (dev < 0 || dev >= kNoallocMaxDevices) return DMPC_ERR_UNSUPPORTED;
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_device_ptr[dev] == nullptr) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || p == nullptr) return DMPC_ERR_CUDA;
+      g_noalloc_device_ptr[dev] = p;
+    }
+    base = g_noalloc_device_ptr[dev];
+  }
+  return launch_common(false, n_groups, groups, nullptr, params, base, (size_t)DMPC_NOALLOC_SCRATCH_BYTES, stream);
 }
 
 int dmpc_linearize(const dmpc_group* group, const dmpc_solver_params* params, double* As, double* Bs, double* Cs,

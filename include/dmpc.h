@@ -175,6 +175,24 @@ void dmpc_default_params(dmpc_solver_params* params);
 int dmpc_solve_fwd(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free forward solve.  No reference counterpart: the reference (JAX)
+ * never hands out raw device memory.  It exists for callers that cannot call
+ * cudaMalloc at solve time -- a real-time MPC control loop where an allocation may
+ * stall the device for an unbounded time, or a host framework that owns the device
+ * allocator and only lends a stream (e.g. a plugin or custom-call handler).
+ * Same semantics and outputs as dmpc_solve_fwd, but the scratch memory is a fixed
+ * array of DMPC_NOALLOC_SCRATCH_BYTES (32 MiB) inside this library, held on every GPU
+ * that loads the library until the process exits.  Problems that need more scratch
+ * than that (dmpc_workspace_size) are rejected with DMPC_ERR_WORKSPACE and nothing is
+ * launched.  The first call on a device looks up the array's device address with that
+ * device current; make that call before any stream capture.  All calls share the one
+ * array and it keeps the previous call's contents (the solver initialises everything it
+ * reads), so calls that may overlap on the GPU -- on different streams, or from several
+ * host threads -- race and must be serialised by the caller. */
+#define DMPC_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int dmpc_solve_fwd_noalloc(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params,
+                           void* stream);
+
 /* Adjoint solve + gradients at the forward solution held in `groups`
  * (states/controls/dual = z*, lambda*; lin_states/lin_controls = last linearization).
  * One launch for all groups (sqp.py:668-798). */
