@@ -42,7 +42,7 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--horizon", type=int, default=60)
-    ap.add_argument("--pcg-tol", type=float, default=1e-11)
+    ap.add_argument("--pcg-tol", type=float, default=1e-13)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU-baseline sample")
     ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")

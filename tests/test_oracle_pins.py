@@ -4,6 +4,9 @@ assertions (no GPU).
 * notebooks/RL_spacecraft.ipynb cells 5-14: rollout loss of one training step
   -2.8196995973193135 and the weights after one gradient step;
 * notebooks/RL_quadrotor.ipynb cells 5-14: loss -241.93737859418738 (slow);
+* benchmarking/imitation-learning/demonstrations.pkl: cart-pole expert control
+  trajectories written by the reference solver (fixture tests/golden/cartpole_demos.npz,
+  made by tests/golden/make_cartpole_demos.py);
 * tests/test_solver_sqp.py, tests/test_optimal_control.py and
   tests/test_differentiable.py assertions, restated on the oracle.
 
@@ -12,6 +15,7 @@ The notebook inputs are regenerated here with the notebooks' own seeded
 """
 
 import copy
+import os
 
 import numpy as np
 import pytest
@@ -216,3 +220,39 @@ def test_differentiable_matches_central_differences():
             wm[k][i] -= eps
             fd = (float(objective(wp)) - float(objective(wm))) / (2 * eps)
             assert abs(fd - float(w[k].grad[i])) < 1e-3 * (1 + abs(fd)), (k, i)
+
+
+# ---- benchmarking/imitation-learning/demonstrations.pkl (reference solver output) ----
+DEMOS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cartpole_demos.npz")
+
+
+def cartpole_demo_problem():
+    """collect_expert_data.py:21-31: cartpole.yaml, SQP <= 501 iterations, line search, PCG 1e-24."""
+    N = 100
+    p = dict(
+        horizon=N, discretization_resolution=0.05, discretization_scheme=0, initial_state=[0.0, 0, 0.1, 0],
+        final_state=[0.0, 0, 0, 0], reference_state_trajectory=np.zeros((N + 1, 4)),
+        reference_control_trajectory=np.zeros((N + 1, 1)), penalize_control_reference=False,
+        weights_penalization_reference_state_trajectory=[1.0, 2.0, 1.5, 1.0],
+        weights_penalization_final_state=[0.0, 0, 0, 0], weights_penalization_control_squared=[5e-2],
+        masscart=1.0, masspole=0.1, length=0.5, gravity=9.81,
+    )
+    sp = default_solver_params()
+    sp["num_scp_iteration_max"] = 501
+    sp["linesearch"] = True
+    sp["pcg"]["tol_epsilon"] = 1e-24
+    return p, sp
+
+
+def test_cartpole_demonstrations_pin():
+    """The oracle re-solves recorded expert demonstrations to <= 1e-6 relative control error."""
+    d = np.load(DEMOS)
+    idx = [0, 2]
+    p, sp = cartpole_demo_problem()
+    solver = SQPSolver(OptimalControlProblem(make_model("cartpole"), p), params=sp)
+    bp = _batched(p, len(idx), initial_state=torch.tensor(d["x0"][idx]))
+    sol = solver._solve(solver.initial_guess(bp), bp, {})
+    ref = torch.tensor(d["ctrl_traj"][idx])
+    assert torch.equal(sol.status, torch.zeros(len(idx), dtype=torch.int64))
+    for j in range(len(idx)):
+        assert float((sol.controls[j] - ref[j]).abs().max() / ref[j].abs().max()) < 1e-6
