@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU-baseline sample")
     ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
+    ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress"],
+                    help="quadrotor = the headline; the others report the remaining workload shapes")
     return ap.parse_args()
 
 
@@ -146,18 +148,22 @@ def build(args, rank):
     return dyn, st, bt, sp
 
 
-def algorithmic_flops(nx, nu, N, sqp_iters, pcg_iters, adj_pcg_iters, rk4=True):
+def algorithmic_flops(nx, nu, N, B, sqp_iters, pcg_iters, adj_pcg_iters, rk4=True):
     """Algorithmic FLOPs of the reference's dense algorithm for the executed iteration
-    counts: F_pcg = 12 K nx^2 + 10 K nx per PCG iteration, F_setup = K (16 nx^3 + 4 nx^2 nu)
-    per QP assembly, F_lin = N (nx + nu) s F_f per linearization (s = 4 for RK4, F_f = 130
-    flops for the quadrotor state_dot)."""
+    counts (totals over the batch of B instances): F_pcg = 12 K nx^2 + 10 K nx per PCG
+    iteration, F_setup = K (16 nx^3 + 4 nx^2 nu) per QP assembly, F_lin = N (nx + nu) s F_f
+    per linearization (s = 4 for RK4, F_f = 130 flops for the quadrotor state_dot).  The
+    adjoint assembles once per instance.  Also returns the FLOPs the scaled-basis FP32
+    iteration executes, 8 K nx^2 + 12 K nx (two off-diagonal block matvecs, unit diagonal)."""
     K = N + 1
     f_pcg = 12 * K * nx * nx + 10 * K * nx
+    f_pcg_exec = 8 * K * nx * nx + 12 * K * nx
     f_setup = K * (16 * nx**3 + 4 * nx * nx * nu)
     f_lin = N * (nx + nu) * (4 if rk4 else 1) * 130
     fwd = sqp_iters * (f_setup + f_lin) + pcg_iters * f_pcg
-    adj = (f_setup + f_lin) + adj_pcg_iters * f_pcg
-    return fwd, adj, f_pcg
+    adj = B * (f_setup + f_lin) + adj_pcg_iters * f_pcg
+    fwd_exec = sqp_iters * (f_setup + f_lin) + pcg_iters * f_pcg_exec
+    return fwd, adj, f_pcg, fwd_exec
 
 
 def fp32_peak_tflops(torch, lib):
@@ -252,7 +258,7 @@ def run_ours(args):
     sqp_iters = float(sol.num_iter.double().sum())
     pcg_iters = float(sol.num_pcg_iters.double().sum())
     adj_iters = float(solver.last_adjoint_pcg_iters.double().sum()) if solver.last_adjoint_pcg_iters is not None else 0.0
-    f_fwd, f_adj, f_pcg = algorithmic_flops(nx, nu, N, sqp_iters, pcg_iters, adj_iters)
+    f_fwd, f_adj, f_pcg, f_fwd_exec = algorithmic_flops(nx, nu, N, B, sqp_iters, pcg_iters, adj_iters)
     fwd_avg = statistics.mean(fwd_ms)
     peak = fp32_peak_tflops(torch, lib)
     achieved = f_fwd / (fwd_avg * 1e-3) / 1e12
@@ -272,7 +278,9 @@ def run_ours(args):
         "adj_kernel_ms": statistics.mean(adj_ms) if adj_ms else None,
         "pcg_iters_per_instance": pcg_iters / B, "sqp_iters_per_instance": sqp_iters / B,
         "adj_pcg_iters_per_instance": adj_iters / B,
-        "adj_achieved_tflops": (f_adj * B / (statistics.mean(adj_ms) * 1e-3) / 1e12) if adj_ms else None,
+        "adj_achieved_tflops": (f_adj / (statistics.mean(adj_ms) * 1e-3) / 1e12) if adj_ms else None,
+        "executed_flops_per_launch": f_fwd_exec,
+        "executed_tflops": f_fwd_exec / (fwd_avg * 1e-3) / 1e12,
     }
 
     line = {
@@ -432,10 +440,116 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed(fn, steps, warmup):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, out
+
+
+def run_other_workload(args):
+    """Throughput / precision of the non-headline workload shapes (one GPU, one line)."""
+    import numpy as np
+    import torch
+
+    from diffmpc_b200 import OptimalControlProblem, SQPSolver, workloads
+    from diffmpc_b200.batch import solve_groups
+
+    dev = torch.device("cuda", 0)
+    line = {"impl": "ours", "workload": args.workload, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "data": "synthetic"}
+    if args.workload == "attitude":
+        B = args.batch if args.batch != 4096 else 1024
+        dyn, st, bt, sp = workloads.attitude(B=B)
+        res = {}
+        for prec in ("mixed", "fp64"):
+            sp2 = dict(sp, precision=prec)
+            solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp2, device=dev)
+            p = workloads.to_device(bt, dev)
+            ms, sol = _timed(lambda: solver.solve(solver.initial_guess(p), p), args.steps, args.warmup)
+            res[prec] = (ms, sol.controls.detach().cpu(), sol.num_pcg_iters.sum(dim=1).double().mean().item())
+        c64 = res["fp64"][1]
+        line.update(metric="batched forward MPC solves/s, attitude nx=7 N=50 B=%d, 10 SQP, eps 1e-8" % B,
+                    value=B / (res["mixed"][0] * 1e-3), fp64_value=B / (res["fp64"][0] * 1e-3),
+                    pcg_iters_mixed=res["mixed"][2], pcg_iters_fp64=res["fp64"][2],
+                    max_rel_control_diff_mixed_vs_fp64=float((res["mixed"][1] - c64).abs().max() / c64.abs().max()))
+    elif args.workload == "mixed":
+        B = args.batch if args.batch != 4096 else 8192
+        rng = np.random.default_rng(1003)
+        groups = []
+        for which in ("linear", "quadrotor"):
+            if which == "linear":
+                dyn, st, bt, sp = workloads.linear_lti(B=B // 2, nx=12, nu=4, N=100, seed=1013)
+            else:
+                dyn, st, bt, sp = workloads.quadrotor(B=B // 2, N=100, seed=1023)
+            sp["pcg"]["tol_epsilon"] = args.pcg_tol
+            sp["num_scp_iteration_max"] = 15
+            sp["precision"] = args.precision
+            solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp, device=dev)
+            p = workloads.to_device(bt, dev)
+            p["horizons"] = torch.tensor(rng.integers(20, 101, size=B // 2), dtype=torch.int32, device=dev)
+            groups.append((solver, p))
+
+        def step():
+            probs = []
+            for solver, p in groups:
+                w = {"initial_state": p["initial_state"].clone().requires_grad_(True)}
+                probs.append((solver, solver.initial_guess(p), p, w))
+            sols = solve_groups(probs)
+            sum((s.controls[:, 0] ** 2).sum() for s in sols).backward()
+            return sols
+
+        ms, sols = _timed(step, args.steps, args.warmup)
+        iters = torch.cat([s.num_pcg_iters.sum(dim=1) for s in sols]).double().cpu()
+        line.update(metric="fwd+bwd MPC solves/s, 50% linear nx=12 / 50% quadrotor, N~U{20..100}, one launch each",
+                    value=B / (ms * 1e-3), ms_per_step=ms, batch=B,
+                    pcg_iters_per_instance_p50=float(iters.quantile(0.5)),
+                    pcg_iters_per_instance_p99=float(iters.quantile(0.99)),
+                    status_success=int(sum(int((s.status == 0).sum()) for s in sols)))
+    else:  # stress
+        B = args.batch if args.batch != 4096 else 1024
+        dyn, st, bt, sp = workloads.linear_stress(B=B)
+        sp["pcg"]["tol_epsilon"] = args.pcg_tol
+        sp["num_scp_iteration_max"] = 2
+        out = {}
+        for prec in ("mixed", "fp64"):
+            sp2 = dict(sp, precision=prec)
+            solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp2, device=dev)
+            p = workloads.to_device(bt, dev)
+
+            def step():
+                w = {"weights_penalization_reference_state_trajectory":
+                     p["weights_penalization_reference_state_trajectory"].clone().requires_grad_(True)}
+                sol = solver.solve(solver.initial_guess(p), p, w)
+                (sol.controls[:, 0] ** 2).sum().backward()
+                return sol, w
+
+            ms, (sol, w) = _timed(step, args.steps, args.warmup)
+            out[prec] = (ms, sol.controls.detach().cpu(), w["weights_penalization_reference_state_trajectory"].grad.cpu(),
+                         sol.num_pcg_iters.sum(dim=1).double().mean().item())
+        c64, g64 = out["fp64"][1], out["fp64"][2]
+        line.update(metric="fwd+bwd MPC solves/s, linear nx=24 nu=8 N=128, diag Q 1e-3..1e3, B=%d" % B,
+                    value=B / (out["mixed"][0] * 1e-3), fp64_value=B / (out["fp64"][0] * 1e-3),
+                    max_rel_control_diff_mixed_vs_fp64=float((out["mixed"][1] - c64).abs().max() / c64.abs().max()),
+                    max_rel_grad_diff_mixed_vs_fp64=float((out["mixed"][2] - g64).abs().max() / g64.abs().max()),
+                    pcg_iters_mixed=out["mixed"][3], pcg_iters_fp64=out["fp64"][3])
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "quadrotor":
+        run_other_workload(args)
     else:
         run_ours(args)
 

@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdmpc.so")
 
 DMPC_OK = 0
+DMPC_ERR_CUDA = 3
 DMPC_MAX_NX = 32
 DMPC_MAX_NU = 16
 DMPC_MAX_ALPHAS = 8
@@ -25,6 +26,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 EXPORTED_SYMBOLS = (
     "dmpc_abi_version",
     "dmpc_error_string",
+    "dmpc_last_cuda_error",
     "dmpc_workspace_size",
     "dmpc_default_params",
     "dmpc_solve_fwd",
@@ -140,6 +142,8 @@ def load():
     lib.dmpc_abi_version.restype = ctypes.c_int
     lib.dmpc_error_string.restype = ctypes.c_char_p
     lib.dmpc_error_string.argtypes = [ctypes.c_int]
+    lib.dmpc_last_cuda_error.restype = ctypes.c_char_p
+    lib.dmpc_last_cuda_error.argtypes = []
     lib.dmpc_workspace_size.restype = ctypes.c_size_t
     lib.dmpc_workspace_size.argtypes = [ctypes.c_int, ctypes.POINTER(Group), ctypes.POINTER(SolverParams)]
     lib.dmpc_default_params.restype = None
@@ -179,5 +183,8 @@ def load():
 
 def check(rc, what):
     if rc != DMPC_OK:
-        msg = load().dmpc_error_string(rc).decode()
+        lib = load()
+        msg = lib.dmpc_error_string(rc).decode()
+        if rc == DMPC_ERR_CUDA:
+            msg += " " + lib.dmpc_last_cuda_error().decode()
         raise DmpcError(f"{what} failed: {msg} (code {rc})")

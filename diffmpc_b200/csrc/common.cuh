@@ -87,3 +87,40 @@ __device__ inline void warp_spd_inverse(double* L, double* R, int n) {
     __syncwarp();
   }
 }
+
+// Cholesky factor and its inverse for one SPD n x n block (n <= 32) by ONE warp.
+// A (row-major) holds the block on entry; its lower triangle is overwritten by L
+// with A = L L^T.  X (n x n, row-major) receives L^-1, zeros above the diagonal
+// included.  Lane i owns row i of A during the factorisation and column i of X
+// during the forward substitution.  Returns false in every lane if a pivot is not
+// positive and finite (the block is not numerically SPD).
+__device__ inline bool warp_chol_inverse(double* A, double* X, int n) {
+  const int lane = threadIdx.x & 31;
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    const double piv = A[k * n + k];
+    ok = ok && piv > 0.0 && isfinite(piv);
+    const double d = sqrt(piv);
+    __syncwarp();
+    if (lane == k) A[k * n + k] = d;
+    if (lane > k && lane < n) A[lane * n + k] = A[lane * n + k] / d;
+    __syncwarp();
+    if (lane > k && lane < n) {
+      const double lik = A[lane * n + k];
+      for (int j = k + 1; j <= lane; ++j) A[lane * n + j] -= lik * A[j * n + k];
+    }
+    __syncwarp();
+  }
+  if (lane < n) {
+    const int j = lane;
+    for (int i = 0; i < j; ++i) X[i * n + j] = 0.0;
+    X[j * n + j] = 1.0 / A[j * n + j];
+    for (int i = j + 1; i < n; ++i) {
+      double acc = 0.0;
+      for (int k = j; k < i; ++k) acc = fma(A[i * n + k], X[k * n + j], acc);
+      X[i * n + j] = -acc / A[i * n + i];
+    }
+  }
+  __syncwarp();
+  return ok;
+}

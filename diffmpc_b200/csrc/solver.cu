@@ -9,11 +9,13 @@
 // the hardware block scheduler balances uneven instances across the 148 SMs.
 //
 // Precision.  DMPC_PREC_FP64 runs the reference's FP64 PCG recurrence.
-// DMPC_PREC_MIXED keeps the block rows of S and Phi^-1 in FP32 in shared
-// memory, runs the PCG iterations in FP32 (dot products accumulated in FP64)
-// and wraps them in FP64 iterative refinement: the residual gamma - S lambda
-// and the stopping test eta = r^T Phi^-1 r <= eps use the FP64 blocks, so the
-// reference's absolute stopping rule (pcg.py:397-403) is applied in FP64.
+// DMPC_PREC_MIXED runs the PCG iterations in FP32 (dot products accumulated in
+// FP64) in the basis scaled by the Cholesky factors of the diagonal blocks, where
+// S and the block preconditioner Phi^-1 both reduce to the identity plus or minus
+// one off-diagonal block per stage (see pcg_pair_scaled), and wraps them in FP64
+// iterative refinement: the residual gamma - S lambda and the stopping test
+// eta = r^T Phi^-1 r <= eps use the FP64 blocks, so the reference's absolute
+// stopping rule (pcg.py:397-403) is applied in FP64.
 //
 // Storage of the Schur system (compact, symmetric block-tridiagonal):
 //   S row t      = -[phi_{t-1}, theta_t, phi_t^T]          (pcg.py:198-211)
@@ -62,7 +64,7 @@ __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a -
 // ---------------------------------------------------------------- workspace layout
 struct Layout {
   // offsets in doubles
-  size_t A, Bm, C, Qi, Ri, q, r, gam, lam, res, t1, xb, ub, xn, un, fv, th, ph, ti, pm, tmp, contrib;
+  size_t A, Bm, C, Qi, Ri, q, r, gam, lam, res, t1, xb, ub, xn, un, fv, th, ph, ti, pm, tmp, li, contrib;
   size_t n_doubles;
   size_t f32;  // float offset (in floats) after the doubles, FP32 blocks when not in smem
   size_t n_floats;
@@ -100,10 +102,11 @@ __host__ __device__ inline Layout make_layout(int nx, int nu, int N, int ld32, b
   L.ti = take(K * nx * nx);
   L.pm = take((size_t)N * nx * nx + nx * nx);
   L.tmp = take(K * nx * nx);
+  L.li = take(K * nx * nx);
   L.contrib = take((size_t)(n_param_grads > 0 ? (n_param_grads < DMPC_MAX_PARAM_GRADS ? n_param_grads : DMPC_MAX_PARAM_GRADS) : 1) * K);
   L.n_doubles = o;
   L.f32 = 0;
-  L.n_floats = blocks_global ? align_up((size_t)4 * K * nx * ld32, 8) : 0;
+  L.n_floats = blocks_global ? align_up((size_t)K * nx * ld32, 8) : 0;
   L.bytes = align_up(L.n_doubles * 8 + L.n_floats * 4, 256);
   return L;
 }
@@ -121,7 +124,7 @@ __host__ __device__ inline size_t smem_bytes_for(int nx, int N, int precision, b
     b += 5 * K * nx * sizeof(double);
   } else {
     b += align_up(5 * (K + 2) * pad_ld(nx) * sizeof(float), 16);
-    if (blocks_smem) b += (size_t)4 * K * nx * pad_ld(nx) * sizeof(float);
+    if (blocks_smem) b += (size_t)K * nx * pad_ld(nx) * sizeof(float);
   }
   return align_up(b, 16);
 }
@@ -132,8 +135,8 @@ struct Inst {
   double dt;
   const double *x0, *xf, *xref, *uref, *wx, *wu, *wf, *mp;
   double *A, *Bm, *C, *Qi, *Ri, *q, *r, *gam, *lam, *res, *t1, *xb, *ub, *xn, *un, *fv;
-  double *th, *ph, *ti, *pm, *tmp, *contrib;
-  float *th32, *ph32, *ti32, *pm32;
+  double *th, *ph, *ti, *pm, *tmp, *li, *contrib;
+  float* w32;  // scaled-basis off-diagonal blocks W_t (FP32, row stride ld)
 };
 
 __device__ inline Inst make_inst(const DevGroup& G, int i, void* ws, float* smem_blocks) {
@@ -181,16 +184,11 @@ __device__ inline Inst make_inst(const DevGroup& G, int i, void* ws, float* smem
   s.ti = base + L.ti;
   s.pm = base + L.pm;
   s.tmp = base + L.tmp;
+  s.li = base + L.li;
   s.contrib = base + L.contrib;
   const bool use_smem = G.blocks_smem == 1 ||
-                        (G.blocks_smem == 2 && (uint64_t)4 * s.K * nx * s.ld * sizeof(float) <= G.smem_block_budget);
-  float* fb = use_smem ? smem_blocks : reinterpret_cast<float*>(base + L.n_doubles);
-  const size_t dblk = (size_t)s.K * nx * s.ld;  // diagonal blocks of this instance
-  const size_t oblk = (size_t)(s.N + 1) * nx * s.ld;
-  s.th32 = fb;
-  s.ti32 = fb + dblk;
-  s.ph32 = fb + 2 * dblk;
-  s.pm32 = fb + 2 * dblk + oblk;
+                        (G.blocks_smem == 2 && (uint64_t)s.K * nx * s.ld * sizeof(float) <= G.smem_block_budget);
+  s.w32 = use_smem ? smem_blocks : reinterpret_cast<float*>(base + L.n_doubles);
   return s;
 }
 
@@ -359,7 +357,11 @@ __device__ void linearize_cost(const Inst& s, const double* xb, const double* ub
 // phi_t = A_t Q_t^-1 An_{t-1}^T with An_{-1} = I, An = -I (pcg.py:182-196);
 // theta^-1 in FP64; P_t = -theta_t^-1 phi_{t-1} theta_{t-1}^-1 (pcg.py:213-239).
 // Writes FP64 blocks th/ph/ti/pm (row stride nx) and, for the mixed precision
-// path, FP32 copies with row stride ld.
+// path, the scaled-basis blocks li (FP64) and w32 (FP32, row stride ld).
+// Set when a theta block has no Cholesky factor in FP64; the QP solve then runs the
+// FP64 recurrence instead of the scaled FP32 iterations.
+__shared__ int sh_scaled_bad;
+
 __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
   const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
   const int nn = nx * nx;
@@ -415,19 +417,43 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
     s.pm[(size_t)k * nn + e] = -a;
   }
   if (fp32_copy) {
+    // scaled basis of the FP32 PCG: Li_t = L_t^-1 with theta_t = L_t L_t^T (FP64), then
+    // W_t = Li_t phi_{t-1} Li_{t-1}^T (t = 1..N) in FP32 at block t-1; block N is zero
+    __syncthreads();  // the P_t pass above has finished reading tmp
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) sh_scaled_bad = 0;
+    __syncthreads();
+    for (int t = warp; t < K; t += nwarp) {
+      double* Lt = s.tmp + (size_t)t * nn;
+      for (int e = lane; e < nn; e += 32) Lt[e] = s.th[(size_t)t * nn + e];
+      __syncwarp();
+      const bool ok = warp_chol_inverse(Lt, s.li + (size_t)t * nn, nx);
+      if (!ok && lane == 0) sh_scaled_bad = 1;
+    }
+    __syncthreads();
+    // T_t = Li_t phi_{t-1} (t = 1..N) in tmp block t
+    for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
+      const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
+      const double* Lr = s.li + (size_t)(k + 1) * nn + i * nx;
+      const double* Pk = s.ph + (size_t)k * nn + j;
+      double a = 0.0;
+      for (int l = 0; l <= i; ++l) a += Lr[l] * Pk[l * nx];
+      s.tmp[(size_t)(k + 1) * nn + e] = a;
+    }
     __syncthreads();
     const int ld = s.ld;
     const int nl = nx * ld;
     for (int w = threadIdx.x; w < K * nl; w += blockDim.x) {
-      const int t = w / nl, e = w - t * nl, i = e / ld, j = e - i * ld;
-      const size_t src = (size_t)t * nn + i * nx + j;
-      const bool real = j < nx;
-      s.th32[w] = real ? (float)s.th[src] : 0.0f;
-      s.ti32[w] = real ? (float)s.ti[src] : 0.0f;
-      // block N of the off-diagonal sets stays zero: the branch-free stencil reads it
-      // in place of the missing neighbour blocks at t = 0 and t = N
-      s.ph32[w] = (real && t < N) ? (float)s.ph[src] : 0.0f;
-      s.pm32[w] = (real && t < N) ? (float)s.pm[src] : 0.0f;
+      const int k = w / nl, e = w - k * nl, i = e / ld, j = e - i * ld;
+      float v = 0.0f;
+      if (j < nx && k < N) {
+        const double* Tr = s.tmp + (size_t)(k + 1) * nn + i * nx;
+        const double* Lm = s.li + (size_t)k * nn + j * nx;  // (Li_{t-1}^T)[l][j] = Li_{t-1}[j][l]
+        double a = 0.0;
+        for (int l = 0; l <= j; ++l) a += Tr[l] * Lm[l];
+        v = (float)a;
+      }
+      s.w32[w] = v;
     }
   }
   __syncthreads();
@@ -468,49 +494,7 @@ __device__ __forceinline__ double block_sum2(double v, double* red, int& parity)
   return warp_sum(s);
 }
 
-// ---------------------------------------------------------------- compile-time-nx stencils
-// FP32 blocks in shared memory with row stride LD (pad_ld), padded vectors v[t*LD + j].
-// y_t,i = Off_{t-1}[i,:] v_{t-1} + Dg_t[i,:] v_t + Off_t[:,i] v_{t+1}
-template <int NX, int LD>
-__device__ __forceinline__ float stencil32(const float* __restrict__ Dg, const float* __restrict__ Off,
-                                           const float* __restrict__ v, int t, int i, int N) {
-  constexpr int BS = NX * LD;
-  constexpr int NP = (NX + 1) / 2;
-  float a0 = 0.f, a1 = 0.f;
-  {
-    const float2* m = reinterpret_cast<const float2*>(Dg + t * BS + i * LD);
-    const float2* x = reinterpret_cast<const float2*>(v + t * LD);
-#pragma unroll
-    for (int j = 0; j < NP; ++j) {
-      const float2 mm = m[j], xx = x[j];
-      a0 = fmaf(mm.x, xx.x, a0);
-      a1 = fmaf(mm.y, xx.y, a1);
-    }
-  }
-  if (t > 0) {
-    const float2* m = reinterpret_cast<const float2*>(Off + (t - 1) * BS + i * LD);
-    const float2* x = reinterpret_cast<const float2*>(v + (t - 1) * LD);
-#pragma unroll
-    for (int j = 0; j < NP; ++j) {
-      const float2 mm = m[j], xx = x[j];
-      a0 = fmaf(mm.x, xx.x, a0);
-      a1 = fmaf(mm.y, xx.y, a1);
-    }
-  }
-  if (t < N) {
-    const float* c = Off + t * BS + i;
-    const float* x = v + (t + 1) * LD;
-#pragma unroll
-    for (int j = 0; j < NX; ++j) {
-      if (j & 1)
-        a1 = fmaf(c[j * LD], x[j], a1);
-      else
-        a0 = fmaf(c[j * LD], x[j], a0);
-    }
-  }
-  return a0 + a1;
-}
-
+// ---------------------------------------------------------------- compile-time-nx stencil
 // FP64 blocks (workspace, row stride NX), dense vectors v[t*NX + j]
 template <int NX>
 __device__ __forceinline__ double stencil64(const double* __restrict__ Dg, const double* __restrict__ Off,
@@ -621,100 +605,38 @@ __device__ __noinline__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, d
   return PcgOut{it, eta};
 }
 
-// FP32 refinement has stagnated (a refinement step cut eta64 by less than 100x, i.e.
-// kappa * eps32 is too close to 1 for FP32 to make progress): finish the solve with the
-// FP64 recurrence on the FP64 blocks, keeping the vectors in workspace regions that are
-// free during the PCG (t1, xn, C).
+// FP32 refinement is not paying off: a refinement step cut eta64 by less than 1e4 (the
+// residual norm by less than 100x: kappa * eps32 is too close to 1 for the FP32 iterations
+// to reach their target in the true residual), or the FP32 iterations have used half of
+// the pcg.max_iter budget.  Finish the solve with the FP64 recurrence on the FP64 blocks
+// within the remaining budget, keeping the vectors in workspace regions that are free
+// during the PCG (t1, xn, C).
 __device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, double eps, double* red, int& par) {
   const int left = max_iter - it > 1 ? max_iter - it : 1;
   PcgOut o = pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, left, eps, red, par);
   return PcgOut{it + o.it, o.eta};
 }
-constexpr double kStagnation = 1e-2;
+constexpr double kStagnation = 1e-4;
 
-// ---------------------------------------------------------------- PCG, FP32 + FP64 refinement
-// lam (FP64, workspace) in/out.  Outer loop: res = gamma - S64 lam, z = Phi64^-1 res,
-// eta64 = res.z; stop like the reference on eta64; otherwise solve S32 d = res/sqrt(eta64)
-// by FP32 PCG to a relative eta reduction of `inner_rel_tol` and update lam += d sqrt(eta64).
-__device__ __noinline__ PcgOut pcg_mixed(const Inst& s, double* lam, float* rv, float* pv, float* tv, float* uv, float* dv,
-                            int max_iter, double eps, int max_ref, double inner_rel, double* red, int& par) {
-  const int n = s.K * s.nx, nx = s.nx, N = s.N, ld = s.ld;
-  int it = 0;
-  double eta64 = 0.0, prev64 = 0.0;
-  for (int ref = 0;; ++ref) {
-    // FP64 residual and preconditioned norm
-    for (int g = threadIdx.x; g < n; g += blockDim.x)
-      s.res[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lam, g);
-    __syncthreads();
-    double part = 0.0;
-    for (int g = threadIdx.x; g < n; g += blockDim.x)
-      part += s.res[g] * stencil_row<double, double>(s.ti, s.pm, nx, nx, N, s.res, g);
-    eta64 = block_sum(part, red, par);
-    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
-    if (!cont || !(eta64 == eta64)) break;
-    if (ref >= max_ref || (ref > 0 && eta64 > kStagnation * prev64)) return fp64_finish(s, lam, it, max_iter, eps, red, par);
-    prev64 = eta64;
-    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
-    // inner FP32 PCG on S32 d = res * scale, d0 = 0
-    for (int g = threadIdx.x; g < n; g += blockDim.x) {
-      rv[g] = (float)(s.res[g] * scale);
-      dv[g] = 0.0f;
-    }
-    __syncthreads();
-    part = 0.0;
-    for (int g = threadIdx.x; g < n; g += blockDim.x) {
-      const float rt = (float)stencil_row<float, float>(s.ti32, s.pm32, ld, nx, N, rv, g);
-      tv[g] = rt;
-      pv[g] = rt;
-      part += (double)rv[g] * (double)rt;
-    }
-    double eta = block_sum(part, red, par);
-    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
-    int inner = 0;
-    while ((eta > target && it <= max_iter - 1) || inner < 1) {
-      part = 0.0;
-      for (int g = threadIdx.x; g < n; g += blockDim.x) {
-        const float u = -(float)stencil_row<float, float>(s.th32, s.ph32, ld, nx, N, pv, g);
-        uv[g] = u;
-        part += (double)pv[g] * (double)u;
-      }
-      const double vden = block_sum(part, red, par);
-      const float alpha = (float)(eta / vden);
-      for (int g = threadIdx.x; g < n; g += blockDim.x) {
-        dv[g] += alpha * pv[g];
-        rv[g] -= alpha * uv[g];
-      }
-      __syncthreads();
-      part = 0.0;
-      for (int g = threadIdx.x; g < n; g += blockDim.x) {
-        const float rt = (float)stencil_row<float, float>(s.ti32, s.pm32, ld, nx, N, rv, g);
-        tv[g] = rt;
-        part += (double)rv[g] * (double)rt;
-      }
-      const double etap = block_sum(part, red, par);
-      const float beta = (float)(etap / eta);
-      for (int g = threadIdx.x; g < n; g += blockDim.x) pv[g] = tv[g] + beta * pv[g];
-      eta = etap;
-      ++it;
-      ++inner;
-      __syncthreads();
-      if (!(eta == eta) || !(vden == vden)) break;
-    }
-    const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
-    for (int g = threadIdx.x; g < n; g += blockDim.x) lam[g] += (double)dv[g] * back;
-    __syncthreads();
-  }
-  return PcgOut{it, eta64};
-}
-
-
-// ---------------------------------------------------------------- PCG, FP32 + FP64 refinement, compile-time nx
-// Same algorithm as pcg_mixed.  Each thread owns up to kSlots rows g = tid + k*blockDim;
-// their r, p, z, S p and update d live in registers and only r and p are published
-// to shared memory (padded layout) for the neighbouring block rows.  Four barriers
-// per iteration: after the S p reduction, after the r update, after the Phi^-1 r
-// reduction, after the p update.
-constexpr int kMaxSlots = 4;
+// ---------------------------------------------------------------- PCG, FP32 in a scaled basis + FP64 refinement
+// Scaled basis.  With the FP64 Cholesky factors theta_t = L_t L_t^T (L block diagonal)
+// and lam = L^-T lam^:
+//   S^   = L^-1 S L^-T    = -(I + F^)
+//   Phi^ = L^T Phi^-1 L   =   I - F^        (Phi^-1 = Theta^-1 - Theta^-1 F Theta^-1)
+// where F is the off-diagonal part of -S (F_{t,t-1} = phi_{t-1}, F_{t,t+1} = phi_t^T) and
+// F^ = L^-1 F L^-T has the blocks F^_{t,t-1} = W_t = L_t^-1 phi_{t-1} L_{t-1}^-T and
+// F^_{t,t+1} = W_{t+1}^T.  PCG is invariant under this congruence (r^ = L^-1 r,
+// z^ = L^T z, p^ = L^T p, S^ p^ = L^-1 S p), so r.z, p.Sp, alpha, beta and eta are those
+// of the reference recurrence (pcg.py:350-436) in exact arithmetic, while an iteration
+// reads only the W blocks: one off-diagonal block per stage instead of the six blocks
+// per knot of S and Phi^-1, and the unit diagonal needs no storage.
+//
+// Refinement (FP64, workspace): res = gamma - S lam and eta64 = res^T Phi^-1 res from the
+// FP64 blocks; stop like the reference on eta64 (pcg.py:397-403); otherwise run the FP32
+// PCG on S^ d^ = L^-1 res / sqrt(eta64) to a relative eta reduction of `inner_rel_tol`
+// (and to 0.01 eps in absolute terms) and update lam += sqrt(eta64) L^-T d^.  A
+// refinement that cuts eta64 by less than 100x, or the max_ref-th refinement, hands the
+// solve to the FP64 recurrence (fp64_finish).
 
 // the kernels' dynamic shared memory, visible to device functions: pointers rebuilt
 // from it let the compiler use shared-space loads instead of generic ones
@@ -748,145 +670,118 @@ __device__ __forceinline__ double fp64_residual(const Inst& s, const double* lam
   return part;
 }
 
-// One stencil row of a block-tridiagonal FP32 operator with every pointer precomputed:
-// dg = Dg_t row i, lo = Off_{t-1} row i (zero block at t = 0), up = Off_t column i
-// (zero block at t = N); vt/vm/vp = v_t, v_{t-1}, v_{t+1} (zero segments past the ends).
-template <int NX, int LD>
-__device__ __forceinline__ float row32(const float* __restrict__ dg, const float* __restrict__ lo,
-                                       const float* __restrict__ up, const float* __restrict__ vt,
-                                       const float* __restrict__ vm, const float* __restrict__ vp) {
-  constexpr int NP = (NX + 1) / 2;
-  const float2* d2 = reinterpret_cast<const float2*>(dg);
-  const float2* l2 = reinterpret_cast<const float2*>(lo);
-  const float2* t2 = reinterpret_cast<const float2*>(vt);
-  const float2* m2 = reinterpret_cast<const float2*>(vm);
-  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-#pragma unroll
-  for (int j = 0; j < NP; ++j) {
-    const float2 md = d2[j], xd = t2[j], ml = l2[j], xl = m2[j];
-    a0 = fmaf(md.x, xd.x, a0);
-    a1 = fmaf(md.y, xd.y, a1);
-    a0 = fmaf(ml.x, xl.x, a0);
-    a1 = fmaf(ml.y, xl.y, a1);
-  }
-#pragma unroll
-  for (int j = 0; j < NX; ++j) a2 = fmaf(up[j * LD], vp[j], a2);
-  return (a0 + a1) + a2;
+// (L_t^-1 v_t)_i = sum_{j <= i} Li_t[i][j] v_t[j]   (FP64 vector with row stride nx)
+__device__ __forceinline__ double lower_row(const double* __restrict__ li, int nx, int t, int i,
+                                            const double* __restrict__ v) {
+  const double* m = li + ((size_t)t * nx + i) * nx;
+  const double* x = v + (size_t)t * nx;
+  double a = 0.0;
+  for (int j = 0; j <= i; ++j) a = fma(m[j], x[j], a);
+  return a;
 }
 
-// FP32 PCG with FP64 iterative refinement (same algorithm as pcg_mixed), for
-// compile-time nx and FP32 blocks in shared memory.  Each thread owns up to kSlots
-// rows g = tid + k*blockDim with their block pointers precomputed once; r, p, z and
-// S p of its rows stay in registers and only r and p are published (padded layout,
-// zero segments before the first and after the last knot) for the neighbouring rows.
-template <int NX, int kSlots>
-__device__ __noinline__ PcgOut pcg_mixed_fast(const Inst& s, double* lam, float* vec, int max_iter, double eps, int max_ref,
-                                              double inner_rel, double* red, int& par) {
-  constexpr int LD = pad_ld(NX);
-  constexpr int BS = NX * LD;
-  const int K = s.K, N = s.N, n = K * NX;
-  float* rbase = as_shared(vec);  // (K + 2) segments: [0][r_0 .. r_N][0]
-  float* pbase = as_shared(vec + (K + 2) * LD);
-  float* rv = rbase + LD;
-  float* pv = pbase + LD;
-  const float* th32 = as_shared(s.th32);
-  const float* ph32 = as_shared(s.ph32);
-  const float* ti32 = as_shared(s.ti32);
-  const float* pm32 = as_shared(s.pm32);
-  int tt[kSlots], ii[kSlots], off[kSlots];
-  bool ok[kSlots];
-  const float *sd[kSlots], *sl[kSlots], *su[kSlots], *md[kSlots], *ml[kSlots], *mu[kSlots];
-#pragma unroll
-  for (int k = 0; k < kSlots; ++k) {
-    const int g = threadIdx.x + k * blockDim.x;
-    ok[k] = g < n;
-    const int t = ok[k] ? g / NX : 0;
-    const int i = ok[k] ? g - t * NX : 0;
-    tt[k] = t;
-    ii[k] = i;
-    off[k] = t * LD + i;
-    const int lo = (t > 0 ? t - 1 : N) * BS + i * LD;  // block N is zero
-    const int up = (t < N ? t : N) * BS + i;
-    sd[k] = th32 + t * BS + i * LD;
-    sl[k] = ph32 + lo;
-    su[k] = ph32 + up;
-    md[k] = ti32 + t * BS + i * LD;
-    ml[k] = pm32 + lo;
-    mu[k] = pm32 + up;
+// (L_t^-T v_t)_i = sum_{j >= i} Li_t[j][i] v_t[j]   (v_t: one FP32 vector segment)
+__device__ __forceinline__ double lower_col(const double* __restrict__ li, int nx, int t, int i,
+                                            const float* __restrict__ vt) {
+  const double* m = li + (size_t)t * nx * nx + i;
+  double a = 0.0;
+  for (int j = i; j < nx; ++j) a = fma(m[(size_t)j * nx], (double)vt[j], a);
+  return a;
+}
+
+// (F^ v)_{t,i} = W_t[i,:] v_{t-1} + W_{t+1}[:,i] v_{t+1} for padded vectors (zero segments
+// at t = -1 and t = K); block N of w is zero and stands in for W_0 and W_{N+1}.
+__device__ __forceinline__ float fhat_row(const float* __restrict__ w, int nx, int ld, int N, int t, int i,
+                                          const float* __restrict__ v) {
+  const int bs = nx * ld;
+  const float* lo = w + (t > 0 ? t - 1 : N) * bs + i * ld;
+  const float* up = w + (t < N ? t : N) * bs + i;
+  const float* vm = v + (t - 1) * ld;
+  const float* vp = v + (t + 1) * ld;
+  float a0 = 0.f, a1 = 0.f;
+  for (int j = 0; j < nx; ++j) {
+    a0 = fmaf(lo[j], vm[j], a0);
+    a1 = fmaf(up[j * ld], vp[j], a1);
   }
-  for (int w = threadIdx.x; w < (K + 2) * LD; w += blockDim.x) {
-    // end segments and padding columns are read by the stencil and must stay zero
-    if (w < LD || w >= (K + 1) * LD || (w % LD) >= NX) {
-      rbase[w] = 0.f;
-      pbase[w] = 0.f;
-    }
-  }
-  float r[kSlots], p[kSlots], d[kSlots], z[kSlots], u[kSlots];
+  return a0 + a1;
+}
+
+// Any nx and horizon: thread rows g = tid + k*blockDim; five padded FP32 vectors
+// (K + 2 segments of ld floats with zero end segments) in shared memory, the W blocks
+// in shared or global memory.
+__device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, float* vec, int max_iter, double eps,
+                                                int max_ref, double inner_rel, double* red, int& par) {
+  const int nx = s.nx, N = s.N, K = s.K, ld = s.ld, n = K * nx;
+  const int span = (K + 2) * ld;
+  for (int w = threadIdx.x; w < 5 * span; w += blockDim.x) vec[w] = 0.f;
+  float* rv = vec + ld;
+  float* pv = rv + span;
+  float* zv = pv + span;
+  float* uv = zv + span;
+  float* dv = uv + span;
+  const float* w32 = s.w32;
   int it = 0;
+  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
   double eta64 = 0.0, prev64 = 0.0;
   for (int ref = 0;; ++ref) {
-    eta64 = block_sum2(fp64_residual<NX, kSlots>(s, lam, tt, ii, ok, N), red, par);
-    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
-    if (!cont || !(eta64 == eta64)) break;
-    if (ref >= max_ref || (ref > 0 && eta64 > kStagnation * prev64)) return fp64_finish(s, lam, it, max_iter, eps, red, par);
-    prev64 = eta64;
-    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
-#pragma unroll
-    for (int k = 0; k < kSlots; ++k)
-      if (ok[k]) {
-        r[k] = (float)(s.res[tt[k] * NX + ii[k]] * scale);
-        d[k] = 0.f;
-        rv[off[k]] = r[k];
-      }
+    for (int g = threadIdx.x; g < n; g += blockDim.x)
+      s.res[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lam, g);
     __syncthreads();
     double part = 0.0;
-#pragma unroll
-    for (int k = 0; k < kSlots; ++k)
-      if (ok[k]) {
-        const float* v = rv + off[k] - ii[k];
-        z[k] = row32<NX, LD>(md[k], ml[k], mu[k], v, v - LD, v + LD);
-        p[k] = z[k];
-        pv[off[k]] = p[k];
-        part += (double)r[k] * (double)z[k];
-      }
-    double eta = block_sum2(part, red, par);
+    for (int g = threadIdx.x; g < n; g += blockDim.x)
+      part += s.res[g] * stencil_row<double, double>(s.ti, s.pm, nx, nx, N, s.res, g);
+    eta64 = block_sum(part, red, par);
+    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
+    if (!cont || !(eta64 == eta64)) break;
+    if (ref >= max_ref || it >= it_cap || (ref > 0 && eta64 > kStagnation * prev64))
+      return fp64_finish(s, lam, it, max_iter, eps, red, par);
+    prev64 = eta64;
+    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx, i = g - t * nx, x = t * ld + i;
+      rv[x] = (float)(scale * lower_row(s.li, nx, t, i, s.res));
+      dv[x] = 0.f;
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx, i = g - t * nx, x = t * ld + i;
+      const float z = rv[x] - fhat_row(w32, nx, ld, N, t, i, rv);
+      pv[x] = z;
+      part += (double)rv[x] * (double)z;
+    }
+    double eta = block_sum(part, red, par);
     const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
     int inner = 0;
-    while ((eta > target && it <= max_iter - 1) || inner < 1) {
+    while ((eta > target && it < it_cap) || inner < 1) {
       part = 0.0;
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k)
-        if (ok[k]) {
-          const float* v = pv + off[k] - ii[k];
-          u[k] = -row32<NX, LD>(sd[k], sl[k], su[k], v, v - LD, v + LD);
-          part += (double)p[k] * (double)u[k];
-        }
-      const double vden = block_sum2(part, red, par);
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const int t = g / nx, i = g - t * nx, x = t * ld + i;
+        const float u = -(pv[x] + fhat_row(w32, nx, ld, N, t, i, pv));
+        uv[x] = u;
+        part += (double)pv[x] * (double)u;
+      }
+      const double vden = block_sum(part, red, par);
       const float alpha = (float)(eta / vden);
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k)
-        if (ok[k]) {
-          d[k] = fmaf(alpha, p[k], d[k]);
-          r[k] = fmaf(-alpha, u[k], r[k]);
-          rv[off[k]] = r[k];
-        }
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const int t = g / nx, x = t * ld + (g - t * nx);
+        dv[x] = fmaf(alpha, pv[x], dv[x]);
+        rv[x] = fmaf(-alpha, uv[x], rv[x]);
+      }
       __syncthreads();
       part = 0.0;
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k)
-        if (ok[k]) {
-          const float* v = rv + off[k] - ii[k];
-          z[k] = row32<NX, LD>(md[k], ml[k], mu[k], v, v - LD, v + LD);
-          part += (double)r[k] * (double)z[k];
-        }
-      const double etap = block_sum2(part, red, par);
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const int t = g / nx, i = g - t * nx, x = t * ld + i;
+        const float z = rv[x] - fhat_row(w32, nx, ld, N, t, i, rv);
+        zv[x] = z;
+        part += (double)rv[x] * (double)z;
+      }
+      const double etap = block_sum(part, red, par);
       const float beta = (float)(etap / eta);
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k)
-        if (ok[k]) {
-          p[k] = fmaf(beta, p[k], z[k]);
-          pv[off[k]] = p[k];
-        }
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const int t = g / nx, x = t * ld + (g - t * nx);
+        pv[x] = fmaf(beta, pv[x], zv[x]);
+      }
       eta = etap;
       ++it;
       ++inner;
@@ -894,37 +789,26 @@ __device__ __noinline__ PcgOut pcg_mixed_fast(const Inst& s, double* lam, float*
       if (!(eta == eta) || !(vden == vden)) break;
     }
     const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
-#pragma unroll
-    for (int k = 0; k < kSlots; ++k)
-      if (ok[k]) lam[tt[k] * NX + ii[k]] += (double)d[k] * back;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx, i = g - t * nx;
+      lam[g] += back * lower_col(s.li, nx, t, i, dv + t * ld);
+    }
     __syncthreads();
   }
   return PcgOut{it, eta64};
 }
 
-// ---------------------------------------------------------------- PCG, FP32 + FP64 refinement, row pairs
-// Same algorithm as pcg_mixed_fast.  Thread (t, q) owns the two rows i0 = q and
-// i1 = q + H (H = ceil(nx/2); i1 exists when q + H < nx) of block row t.  The S
-// coefficients of both rows (2 x 3 x nx floats) are held in registers for the whole
-// QP solve, so the S matvec reads only the vector from shared memory; every vector
-// segment is loaded once per thread and used for both rows.  Phi^-1 stays in shared
-// memory.  Needs K * H <= blockDim.
+// Compile-time nx, K * ceil(nx/2) <= blockDim.  Thread (t, q) = (tid mod K, tid div K) owns
+// the rows i0 = q and i1 = q + H (H = ceil(nx/2); i1 exists when q + H < nx) of block row t
+// and keeps their W coefficients (W_t rows i0, i1 and W_{t+1} columns i0, i1: 4 nx floats)
+// in registers for the whole QP solve.  Both operators then read only the vector
+// segments t-1 and t+1 from shared memory, each loaded once for both rows.  Lanes run
+// over t for a fixed q, so a half warp's 64-bit segment loads (ld/2 odd) hit distinct
+// banks.  Threads past the last pair (tid >= H K) idle on row 0 of block 0, which keeps
+// every address in range; they take part in the barriers and reductions with zeros.
 template <int NX>
-__device__ __forceinline__ void load_row_regs(const float* __restrict__ dg, const float* __restrict__ lo,
-                                              const float* __restrict__ up, float (&d)[NX], float (&l)[NX],
-                                              float (&u)[NX]) {
-  constexpr int LD = pad_ld(NX);
-#pragma unroll
-  for (int j = 0; j < NX; ++j) {
-    d[j] = dg[j];
-    l[j] = lo[j];
-    u[j] = up[j * LD];
-  }
-}
-
-template <int NX>
-__device__ __noinline__ PcgOut pcg_mixed_pair(const Inst& s, double* lam, float* vec, int max_iter, double eps,
-                                              int max_ref, double inner_rel, double* red, int& par) {
+__device__ __noinline__ PcgOut pcg_pair_scaled(const Inst& s, double* lam, float* vec, int max_iter, double eps,
+                                               int max_ref, double inner_rel, double* red, int& par) {
   constexpr int LD = pad_ld(NX);
   constexpr int BS = NX * LD;
   constexpr int H = (NX + 1) / 2;
@@ -934,26 +818,25 @@ __device__ __noinline__ PcgOut pcg_mixed_pair(const Inst& s, double* lam, float*
   float* pbase = as_shared(vec + (K + 2) * LD);
   float* rv = rbase + LD;
   float* pv = pbase + LD;
-  const float* ti32 = as_shared(s.ti32);
-  const float* pm32 = as_shared(s.pm32);
-  const int t = threadIdx.x / H;
-  const int q = threadIdx.x - t * H;
-  const bool ok0 = t < K;
+  const int qq = threadIdx.x / K;
+  const bool ok0 = qq < H;
+  const int q = ok0 ? qq : 0;
+  const int tc = ok0 ? threadIdx.x - qq * K : 0;
   const bool ok1 = ok0 && (q + H < NX);
-  const int tc = ok0 ? t : 0;
   const int i0 = q, i1 = ok1 ? q + H : q;
-  const int lo_blk = (tc > 0 ? tc - 1 : N) * BS;  // block N of the off-diagonal sets is zero
+  const int lo_blk = (tc > 0 ? tc - 1 : N) * BS;  // block N is zero
   const int up_blk = (tc < N ? tc : N) * BS;
-  // S rows in registers (FP32 blocks may live in shared or global memory)
-  float sd0[NX], sl0[NX], su0[NX], sd1[NX], sl1[NX], su1[NX];
-  load_row_regs<NX>(s.th32 + tc * BS + i0 * LD, s.ph32 + lo_blk + i0 * LD, s.ph32 + up_blk + i0, sd0, sl0, su0);
-  load_row_regs<NX>(s.th32 + tc * BS + i1 * LD, s.ph32 + lo_blk + i1 * LD, s.ph32 + up_blk + i1, sd1, sl1, su1);
-  const float* md0 = ti32 + tc * BS + i0 * LD;
-  const float* ml0 = pm32 + lo_blk + i0 * LD;
-  const float* mu0 = pm32 + up_blk + i0;
-  const float* md1 = ti32 + tc * BS + i1 * LD;
-  const float* ml1 = pm32 + lo_blk + i1 * LD;
-  const float* mu1 = pm32 + up_blk + i1;
+  float wl0[NX], wl1[NX], wu0[NX], wu1[NX];
+  {
+    const float* w = s.w32;
+#pragma unroll
+    for (int j = 0; j < NX; ++j) {
+      wl0[j] = w[lo_blk + i0 * LD + j];
+      wl1[j] = w[lo_blk + i1 * LD + j];
+      wu0[j] = w[up_blk + j * LD + i0];
+      wu1[j] = w[up_blk + j * LD + i1];
+    }
+  }
   const int seg = tc * LD;  // segment t in the padded vectors
   for (int w = threadIdx.x; w < (K + 2) * LD; w += blockDim.x) {
     if (w < LD || w >= (K + 1) * LD || (w % LD) >= NX) {
@@ -961,99 +844,64 @@ __device__ __noinline__ PcgOut pcg_mixed_pair(const Inst& s, double* lam, float*
       pbase[w] = 0.f;
     }
   }
+  // F^ v for the two rows
+  auto fhat = [&](const float* v, float& f0, float& f1) {
+    const float2* vm = reinterpret_cast<const float2*>(v + seg - LD);
+    const float2* vp = reinterpret_cast<const float2*>(v + seg + LD);
+    float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      const float2 y = vm[j], x = vp[j];
+      const int j0 = 2 * j, j1 = 2 * j + 1;
+      a0 = fmaf(wl0[j0], y.x, a0);
+      a1 = fmaf(wl1[j0], y.x, a1);
+      a0 = fmaf(wu0[j0], x.x, a0);
+      a1 = fmaf(wu1[j0], x.x, a1);
+      if (j1 < NX) {
+        b0 = fmaf(wl0[j1], y.y, b0);
+        b1 = fmaf(wl1[j1], y.y, b1);
+        b0 = fmaf(wu0[j1], x.y, b0);
+        b1 = fmaf(wu1[j1], x.y, b1);
+      }
+    }
+    f0 = a0 + b0;
+    f1 = a1 + b1;
+  };
   int tt[2] = {tc, tc}, ii[2] = {i0, i1};
   bool ok[2] = {ok0, ok1};
   float r0 = 0.f, r1 = 0.f, p0 = 0.f, p1 = 0.f, d0 = 0.f, d1 = 0.f;
   int it = 0;
+  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
   double eta64 = 0.0, prev64 = 0.0;
   for (int ref = 0;; ++ref) {
     eta64 = block_sum2(fp64_residual<NX, 2>(s, lam, tt, ii, ok, N), red, par);
     const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
     if (!cont || !(eta64 == eta64)) break;
-    if (ref >= max_ref || (ref > 0 && eta64 > kStagnation * prev64)) return fp64_finish(s, lam, it, max_iter, eps, red, par);
+    if (ref >= max_ref || it >= it_cap || (ref > 0 && eta64 > kStagnation * prev64))
+      return fp64_finish(s, lam, it, max_iter, eps, red, par);
     prev64 = eta64;
     const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
     d0 = 0.f;
     d1 = 0.f;
-    if (ok0) {
-      r0 = (float)(s.res[tc * NX + i0] * scale);
-      rv[seg + i0] = r0;
-    }
-    if (ok1) {
-      r1 = (float)(s.res[tc * NX + i1] * scale);
-      rv[seg + i1] = r1;
-    }
+    r0 = ok0 ? (float)(scale * lower_row(s.li, NX, tc, i0, s.res)) : 0.f;
+    r1 = ok1 ? (float)(scale * lower_row(s.li, NX, tc, i1, s.res)) : 0.f;
+    if (ok0) rv[seg + i0] = r0;
+    if (ok1) rv[seg + i1] = r1;
     __syncthreads();
-    // z = Phi^-1 r for the two rows (shared-memory matrix, vector segments loaded once)
-    auto precond = [&](float& z0, float& z1) {
-      float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
-      const float2* vt = reinterpret_cast<const float2*>(rv + seg);
-      const float2* vm = reinterpret_cast<const float2*>(rv + seg - LD);
-      const float2* d20 = reinterpret_cast<const float2*>(md0);
-      const float2* d21 = reinterpret_cast<const float2*>(md1);
-      const float2* l20 = reinterpret_cast<const float2*>(ml0);
-      const float2* l21 = reinterpret_cast<const float2*>(ml1);
-#pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const float2 x = vt[j], y = vm[j];
-        const float2 m0 = d20[j], m1 = d21[j], n0 = l20[j], n1 = l21[j];
-        a0 = fmaf(m0.x, x.x, a0);
-        b0 = fmaf(m0.y, x.y, b0);
-        a1 = fmaf(m1.x, x.x, a1);
-        b1 = fmaf(m1.y, x.y, b1);
-        a0 = fmaf(n0.x, y.x, a0);
-        b0 = fmaf(n0.y, y.y, b0);
-        a1 = fmaf(n1.x, y.x, a1);
-        b1 = fmaf(n1.y, y.y, b1);
-      }
-      const float* vp = rv + seg + LD;
-#pragma unroll
-      for (int j = 0; j < NX; ++j) {
-        const float x = vp[j];
-        a0 = fmaf(mu0[j * LD], x, a0);
-        a1 = fmaf(mu1[j * LD], x, a1);
-      }
-      z0 = a0 + b0;
-      z1 = a1 + b1;
-    };
-    float z0, z1;
-    precond(z0, z1);
-    p0 = z0;
-    p1 = z1;
+    float f0, f1;
+    fhat(rv, f0, f1);
+    p0 = r0 - f0;
+    p1 = r1 - f1;
     if (ok0) pv[seg + i0] = p0;
     if (ok1) pv[seg + i1] = p1;
-    double part = (ok0 ? (double)r0 * (double)z0 : 0.0) + (ok1 ? (double)r1 * (double)z1 : 0.0);
+    double part = (ok0 ? (double)r0 * (double)p0 : 0.0) + (ok1 ? (double)r1 * (double)p1 : 0.0);
     double eta = block_sum2(part, red, par);
     const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
     int inner = 0;
-    while ((eta > target && it <= max_iter - 1) || inner < 1) {
-      // u = S p = -(phi_{t-1} p_{t-1} + theta_t p_t + phi_t^T p_{t+1}), coefficients in registers
-      float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
-      {
-        const float2* vt = reinterpret_cast<const float2*>(pv + seg);
-        const float2* vm = reinterpret_cast<const float2*>(pv + seg - LD);
-        const float2* vq = reinterpret_cast<const float2*>(pv + seg + LD);
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-          const float2 x = vt[j], y = vm[j], w = vq[j];
-          const int j0 = 2 * j, j1 = 2 * j + 1;
-          a0 = fmaf(sd0[j0], x.x, a0);
-          a1 = fmaf(sd1[j0], x.x, a1);
-          a0 = fmaf(sl0[j0], y.x, a0);
-          a1 = fmaf(sl1[j0], y.x, a1);
-          a0 = fmaf(su0[j0], w.x, a0);
-          a1 = fmaf(su1[j0], w.x, a1);
-          if (j1 < NX) {
-            b0 = fmaf(sd0[j1], x.y, b0);
-            b1 = fmaf(sd1[j1], x.y, b1);
-            b0 = fmaf(sl0[j1], y.y, b0);
-            b1 = fmaf(sl1[j1], y.y, b1);
-            b0 = fmaf(su0[j1], w.y, b0);
-            b1 = fmaf(su1[j1], w.y, b1);
-          }
-        }
-      }
-      const float u0 = -(a0 + b0), u1 = -(a1 + b1);
+    while ((eta > target && it < it_cap) || inner < 1) {
+      // u^ = S^ p^ = -(p^ + F^ p^)
+      fhat(pv, f0, f1);
+      const float u0 = -(p0 + f0), u1 = -(p1 + f1);
       part = (ok0 ? (double)p0 * (double)u0 : 0.0) + (ok1 ? (double)p1 * (double)u1 : 0.0);
       const double vden = block_sum2(part, red, par);
       const float alpha = (float)(eta / vden);
@@ -1064,7 +912,9 @@ __device__ __noinline__ PcgOut pcg_mixed_pair(const Inst& s, double* lam, float*
       if (ok0) rv[seg + i0] = r0;
       if (ok1) rv[seg + i1] = r1;
       __syncthreads();
-      precond(z0, z1);
+      // z^ = Phi^ r^ = r^ - F^ r^
+      fhat(rv, f0, f1);
+      const float z0 = r0 - f0, z1 = r1 - f1;
       part = (ok0 ? (double)r0 * (double)z0 : 0.0) + (ok1 ? (double)r1 * (double)z1 : 0.0);
       const double etap = block_sum2(part, red, par);
       const float beta = (float)(etap / eta);
@@ -1078,9 +928,13 @@ __device__ __noinline__ PcgOut pcg_mixed_pair(const Inst& s, double* lam, float*
       __syncthreads();
       if (!(eta == eta) || !(vden == vden)) break;
     }
+    // lam += sqrt(eta64) L^-T d^, with d^ published over r^ (no thread reads r^ any more)
+    if (ok0) rv[seg + i0] = d0;
+    if (ok1) rv[seg + i1] = d1;
+    __syncthreads();
     const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
-    if (ok0) lam[tc * NX + i0] += (double)d0 * back;
-    if (ok1) lam[tc * NX + i1] += (double)d1 * back;
+    if (ok0) lam[tc * NX + i0] += back * lower_col(s.li, NX, tc, i0, rv + seg);
+    if (ok1) lam[tc * NX + i1] += back * lower_col(s.li, NX, tc, i1, rv + seg);
     __syncthreads();
   }
   return PcgOut{it, eta64};
@@ -1276,47 +1130,25 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
     return o;
   }
   float* v = reinterpret_cast<float*>(sv.vec);
-  if (s.th32 == sv.blocks && s.K * ((s.nx + 1) / 2) <= (int)blockDim.x) {
+  if (sh_scaled_bad) return fp64_finish(s, lam, 0, P.pcg_max_iter, P.pcg_tol_epsilon, sv.red, par);
+  if (s.K * ((s.nx + 1) / 2) <= (int)blockDim.x) {
     switch (s.nx) {
 #define DMPC_PAIR(NXV)                                                                                   \
   case NXV:                                                                                              \
-    return pcg_mixed_pair<NXV>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,           \
-                               P.inner_rel_tol, sv.red, par);
+    return pcg_pair_scaled<NXV>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,          \
+                                P.inner_rel_tol, sv.red, par);
       DMPC_PAIR(3)
       DMPC_PAIR(4)
+      DMPC_PAIR(6)
       DMPC_PAIR(7)
       DMPC_PAIR(12)
       DMPC_PAIR(13)
-      DMPC_PAIR(24)
 #undef DMPC_PAIR
       default: break;
     }
   }
-  if (s.th32 == sv.blocks && n <= kMaxSlots * (int)blockDim.x) {
-    const int slots = (n + blockDim.x - 1) / blockDim.x;
-    switch (s.nx) {
-#define DMPC_FAST(NXV)                                                                                  \
-  case NXV:                                                                                             \
-    if (slots == 1)                                                                                     \
-      return pcg_mixed_fast<NXV, 1>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,     \
-                                    P.inner_rel_tol, sv.red, par);                                      \
-    if (slots == 2)                                                                                     \
-      return pcg_mixed_fast<NXV, 2>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,     \
-                                    P.inner_rel_tol, sv.red, par);                                      \
-    return pcg_mixed_fast<NXV, 4>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement,       \
-                                  P.inner_rel_tol, sv.red, par);
-      DMPC_FAST(3)
-      DMPC_FAST(4)
-      DMPC_FAST(7)
-      DMPC_FAST(12)
-      DMPC_FAST(13)
-      DMPC_FAST(24)
-#undef DMPC_FAST
-      default: break;
-    }
-  }
-  return pcg_mixed(s, lam, v, v + n, v + 2 * n, v + 3 * n, v + 4 * n, P.pcg_max_iter, P.pcg_tol_epsilon,
-                   P.max_refinement, P.inner_rel_tol, sv.red, par);
+  return pcg_mixed_scaled(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement, P.inner_rel_tol,
+                          sv.red, par);
 }
 
 // ---------------------------------------------------------------- forward kernel
@@ -1804,7 +1636,7 @@ __global__ void __launch_bounds__(256) k_pcg_dense(int N, int nx, int nu, const 
                                                    int max_iter, double eps, double* lam_out, double* xs,
                                                    double* us, int32_t* iters, double* etas) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int b = blockIdx.x, K = N + 1, n = K * nx, nn = nx * nx;
+  const int b = blockIdx.x, K = N + 1, n = K * nx;
   double* red = reinterpret_cast<double*>(smem);
   double* lv = red + 128;
   double *rv = lv + n, *pv = rv + n, *tv = pv + n, *uv = tv + n;
@@ -1880,16 +1712,31 @@ __global__ void __launch_bounds__(256) k_fma_probe(int iters, float seed, float*
 }
 
 // ---------------------------------------------------------------- host side
-bool fast_nx(int nx) { return nx == 3 || nx == 4 || nx == 7 || nx == 12 || nx == 13 || nx == 24; }
+// Last CUDA error seen by an entry point on this thread (dmpc_last_cuda_error).
+thread_local cudaError_t g_last_cuda_error = cudaSuccess;
+int cuda_rc(cudaError_t e) {
+  if (e == cudaSuccess) return DMPC_OK;
+  g_last_cuda_error = e;
+  return DMPC_ERR_CUDA;
+}
 
-// Threads per CTA (<= 512, the kernels' launch bound).  Mixed precision with shared-memory
-// blocks: one thread per row pair when K * ceil(nx/2) fits, else one thread per row up to
-// 512 threads (several rows per thread beyond that).
-int choose_threads(const dmpc_solver_params* p, int nx, int K, bool blocks_smem) {
+// Static shared memory of the SQP kernels: the per-instance context (sh_inst) and the
+// scaled-basis flag.  It counts against the same per-CTA opt-in limit as the dynamic
+// request, so every dynamic size is checked against optin - kStaticSmemReserve.  A fixed
+// reserve (checked at compile time) keeps the size logic free of runtime queries.
+constexpr size_t kStaticSmemReserve = 1024;
+static_assert(sizeof(Inst) + 2 * sizeof(int) + 64 <= kStaticSmemReserve, "static shared memory reserve too small");
+
+// nx with a row-pair specialisation of the scaled FP32 PCG (pcg_pair_scaled)
+bool pair_nx(int nx) { return nx == 3 || nx == 4 || nx == 6 || nx == 7 || nx == 12 || nx == 13; }
+
+// Threads per CTA (<= 512, the kernels' launch bound).  Mixed precision: one thread per
+// row pair when K * ceil(nx/2) fits, else one thread per row up to 512 threads (several
+// rows per thread beyond that).
+int choose_threads(const dmpc_solver_params* p, int nx, int K) {
   if (p && p->threads_per_block > 0) return p->threads_per_block;
   int rows = K * nx;
-  if (p && p->precision == DMPC_PREC_MIXED && blocks_smem && fast_nx(nx) && K * ((nx + 1) / 2) <= 512)
-    rows = K * ((nx + 1) / 2);
+  if (p && p->precision == DMPC_PREC_MIXED && pair_nx(nx) && K * ((nx + 1) / 2) <= 512) rows = K * ((nx + 1) / 2);
   int t = ((rows + 31) / 32) * 32;
   if (t < 128) t = 128;
   if (t > 512) t = 512;
@@ -1915,6 +1762,7 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
   if (cudaGetDevice(&dev) == cudaSuccess)
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem_optin <= 0) smem_optin = 227 * 1024;
+  const size_t smem_cap = (size_t)smem_optin - kStaticSmemReserve;
   for (int k = 0; k < n_groups; ++k) {
     const dmpc_group& g = groups[k];
     if (!model_dims_ok(g.model, g.nx, g.nu)) return DMPC_ERR_UNSUPPORTED;
@@ -1933,17 +1781,16 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     const size_t base = smem_bytes_for(g.nx, g.horizon, p->precision, false);
     int mode = 0;
     if (p->precision == DMPC_PREC_MIXED && p->blocks_in_smem != 0) {
-      if (need_all <= (size_t)smem_optin)
+      if (need_all <= smem_cap)
         mode = 1;
-      else if (g.horizons && base + (size_t)8 * g.nx * pad_ld(g.nx) * sizeof(float) <= (size_t)smem_optin)
+      else if (g.horizons && base + (size_t)2 * g.nx * pad_ld(g.nx) * sizeof(float) <= smem_cap)
         mode = 2;
     }
     if (p->blocks_in_smem == 1 && p->precision == DMPC_PREC_MIXED && mode != 1) return DMPC_ERR_UNSUPPORTED;
-    const bool in_smem = mode == 1;
     G.blocks_smem = mode;
-    G.smem_block_budget = mode == 2 ? (uint64_t)smem_optin - base : 0;
-    const size_t sm = mode == 1 ? need_all : (mode == 2 ? (size_t)smem_optin : base);
-    if (sm > (size_t)smem_optin) return DMPC_ERR_UNSUPPORTED;
+    G.smem_block_budget = mode == 2 ? (uint64_t)(smem_cap - base) : 0;
+    const size_t sm = mode == 1 ? need_all : (mode == 2 ? smem_cap : base);
+    if (sm > smem_cap) return DMPC_ERR_UNSUPPORTED;
     if (sm > smax) smax = sm;
     int ng = 0;
     if (adj) {
@@ -1962,7 +1809,7 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     G.ws_stride = L.bytes;
     off += L.bytes * (size_t)g.batch;
     blocks += g.batch;
-    const int t = choose_threads(p, g.nx, G.K, in_smem);
+    const int t = choose_threads(p, g.nx, G.K);
     if (t > thr) thr = t;
   }
   args->total_blocks = blocks;
@@ -1990,6 +1837,8 @@ void* g_noalloc_device_ptr[kNoallocMaxDevices] = {};
 extern "C" {
 
 int dmpc_abi_version(void) { return DMPC_ABI_VERSION; }
+
+const char* dmpc_last_cuda_error(void) { return cudaGetErrorName(g_last_cuda_error); }
 
 const char* dmpc_error_string(int code) {
   switch (code) {
@@ -2064,7 +1913,7 @@ static int launch_common(bool adjoint, int n_groups, const dmpc_group* groups, c
     }
   }
   delete args;
-  return e == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+  return cuda_rc(e);
 }
 
 int dmpc_solve_fwd(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params, void* workspace,
@@ -2091,7 +1940,8 @@ int dmpc_solve_fwd_noalloc(int n_groups, const dmpc_group* groups, const dmpc_so
   if (rc != DMPC_OK) return rc;
   if (need > (size_t)DMPC_NOALLOC_SCRATCH_BYTES) return DMPC_ERR_WORKSPACE;
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess) return DMPC_ERR_CUDA;
+  const cudaError_t de = cudaGetDevice(&dev);
+  if (de != cudaSuccess) return cuda_rc(de);
   if (dev < 0 || dev >= kNoallocMaxDevices) return DMPC_ERR_UNSUPPORTED;
   void* base = nullptr;
   {
@@ -2099,7 +1949,7 @@ int dmpc_solve_fwd_noalloc(int n_groups, const dmpc_group* groups, const dmpc_so
     if (g_noalloc_device_ptr[dev] == nullptr) {
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || p == nullptr) return DMPC_ERR_CUDA;
+      if (e != cudaSuccess || p == nullptr) return cuda_rc(e != cudaSuccess ? e : cudaErrorInvalidSymbol);
       g_noalloc_device_ptr[dev] = p;
     }
     base = g_noalloc_device_ptr[dev];
@@ -2120,7 +1970,8 @@ int dmpc_linearize(const dmpc_group* group, const dmpc_solver_params* params, do
   if (rc == DMPC_OK && args->total_blocks > 0) {
     k_linearize<<<args->total_blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*args, workspace, As, Bs, Cs,
                                                                                         Qinv, qvec, Rinv, rvec);
-    if (cudaGetLastError() != cudaSuccess) rc = DMPC_ERR_CUDA;
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) rc = cuda_rc(le);
   }
   delete args;
   return rc;
@@ -2133,7 +1984,7 @@ int dmpc_compute_gamma(int batch, int N, int nx, int nu, const double* As_x_Qinv
   if (batch == 0) return DMPC_OK;
   k_gamma_dense<<<batch, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(N, nx, nu, As_x_Qinv, Asnext_x_Qinvnext,
                                                                            Bs_x_Rinv, Cs, Q0inv, qvec, rvec, gamma);
-  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+  return cuda_rc(cudaGetLastError());
 }
 
 int dmpc_kkt_recover(int batch, int N, int nx, int nu, const double* lambda, const double* As_next, const double* As,
@@ -2144,10 +1995,10 @@ int dmpc_kkt_recover(int batch, int N, int nx, int nu, const double* lambda, con
   const size_t sm = 2 * (size_t)(N + 1) * nx * sizeof(double);
   if (sm > 227 * 1024) return DMPC_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(k_recover_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return DMPC_ERR_CUDA;
+  if (e != cudaSuccess) return cuda_rc(e);
   k_recover_dense<<<batch, 256, sm, reinterpret_cast<cudaStream_t>(stream)>>>(N, nx, nu, lambda, As_next, As, Bs,
                                                                               Qinv, qvec, Rinv, rvec, states, controls);
-  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+  return cuda_rc(cudaGetLastError());
 }
 
 double dmpc_probe_fp32_fma(int blocks, int iters, float* out, void* stream) {
@@ -2170,7 +2021,7 @@ int dmpc_schur_assemble(int batch, int N, int nx, int nu, const double* As_next,
   if (batch == 0) return DMPC_OK;
   k_schur_dense<<<batch, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       N, nx, nu, As_next, As, Bs, Cs, Qinv, qvec, Rinv, rvec, S, Phiinv, gamma, reinterpret_cast<double*>(workspace));
-  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+  return cuda_rc(cudaGetLastError());
 }
 
 int dmpc_pcg_solve(int batch, int N, int nx, int nu, const double* S, const double* Phiinv, const double* gamma,
@@ -2183,11 +2034,11 @@ int dmpc_pcg_solve(int batch, int N, int nx, int nu, const double* S, const doub
   const size_t sm = 128 * sizeof(double) + 5 * (size_t)(N + 1) * nx * sizeof(double);
   if (sm > 227 * 1024) return DMPC_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(k_pcg_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return DMPC_ERR_CUDA;
+  if (e != cudaSuccess) return cuda_rc(e);
   k_pcg_dense<<<batch, 256, sm, reinterpret_cast<cudaStream_t>(stream)>>>(
       N, nx, nu, S, Phiinv, gamma, lambda_guess, As_next, As, Bs, Qinv, qvec, Rinv, rvec, max_iter, tol_epsilon,
       lambda, states, controls, num_iterations, convergence_eta);
-  return cudaGetLastError() == cudaSuccess ? DMPC_OK : DMPC_ERR_CUDA;
+  return cuda_rc(cudaGetLastError());
 }
 
 }  // extern "C"

@@ -163,6 +163,10 @@ typedef struct dmpc_adjoint {
 
 int dmpc_abi_version(void);
 const char* dmpc_error_string(int code);
+/* Name of the last CUDA runtime error an entry point returned DMPC_ERR_CUDA for on the
+ * calling thread ("cudaSuccess" if none).  No reference counterpart: the reference
+ * surfaces XLA runtime errors as Python exceptions. */
+const char* dmpc_last_cuda_error(void);
 
 /* Bytes of workspace the forward/adjoint calls need for these groups. */
 size_t dmpc_workspace_size(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params);

@@ -86,6 +86,26 @@ def test_host_validation_rejects_bad_descriptors():
     assert lib.dmpc_error_string(2) == b"workspace too small or misaligned"
 
 
+@pytest.mark.timeout(120)
+def test_calls_return_a_named_cuda_error_without_a_device():
+    """With no usable device every entry point returns DMPC_ERR_CUDA promptly (it never
+    blocks) and dmpc_last_cuda_error names the runtime's error."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-device error path")
+    lib = _lib.load()
+    p = _lib.SolverParams()
+    lib.dmpc_default_params(p)
+    n = lib.dmpc_workspace_size(1, _group(), p)
+    fake = 1 << 20  # 256-byte aligned; the failed launch never dereferences it
+    assert lib.dmpc_solve_fwd(1, _group(), p, fake, n, None) == 3
+    assert lib.dmpc_last_cuda_error() not in (b"cudaSuccess", b"")
+    assert lib.dmpc_solve_fwd_noalloc(1, _group(), p, None) == 3
+    with pytest.raises(_lib.DmpcError, match="CUDA runtime error cuda"):
+        _lib.check(3, "dmpc_solve_fwd")
+
+
 def test_workspace_grows_with_batch_and_horizon():
     lib = _lib.load()
     p = _lib.SolverParams()

@@ -4,7 +4,8 @@
   horizons in ONE forward launch (and one adjoint launch).  Each instance is
   checked against the oracle solving it alone with its own horizon.
 * nx=24, N=128 linear with diagonal Q spanning 1e-3..1e3: its FP32 blocks
-  (1.3 MB) do not fit in shared memory and stay in the workspace.
+  (322 KB) do not fit in shared memory and stay in the workspace; in a ragged group
+  each instance places its blocks by its own horizon.
 """
 
 import pytest
@@ -75,6 +76,18 @@ def test_groups_gradients_equal_single_group_solves():
     for a, b in ((wa, wa2), (wq, wq2)):
         for k in a:
             assert rel_err(a[k].grad, b[k].grad) < 1e-10, k
+
+
+def test_ragged_group_places_blocks_per_instance():
+    """nx=24 with horizons 128 and 40: the group's longest instance does not fit in shared
+    memory, so each instance decides at run time (the short one keeps its FP32 blocks on
+    chip, the long one in the workspace)."""
+    dyn, st, bt, sp, solver, p = _group(lambda: workloads.linear_stress(B=2, seed=46), [128, 40], 1e-13)
+    sol = solver.solve(solver.initial_guess(p), p)
+    torch.cuda.synchronize()
+    for i, n in enumerate(p["horizons"].tolist()):
+        o = _instance_oracle(dyn, st, bt, sp, i, n)
+        assert rel_err(sol.controls[i, : n + 1], o.controls[0]) < 1e-6
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
