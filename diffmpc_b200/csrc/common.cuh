@@ -124,3 +124,46 @@ __device__ inline bool warp_chol_inverse(double* A, double* X, int n) {
   __syncwarp();
   return ok;
 }
+
+// Register-resident variant for compile-time NX <= 16: ONE warp factors the SPD block
+// th (NX x NX, row-major) as L L^T and writes X = L^-1 to li (row-major, zeros above the
+// diagonal).  Lane i holds row i of the block, then of L, in registers; the forward
+// substitution gives lane c column c of X.  Every operand crosses lanes by shuffle, so the
+// only memory traffic is one read of th and one coalesced write of X.  Lanes >= NX mirror
+// row 0 and store nothing.  Returns false in every lane if a pivot is not positive and
+// finite.
+template <int NX>
+__device__ __forceinline__ bool warp_chol_inverse_regs(const double* __restrict__ th, double* __restrict__ li) {
+  const int lane = threadIdx.x & 31;
+  const int r = lane < NX ? lane : 0;
+  double a[NX];
+#pragma unroll
+  for (int j = 0; j < NX; ++j) a[j] = th[r * NX + j];
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < NX; ++k) {
+    const double piv = __shfl_sync(DMPC_FULL_MASK, a[k], k);
+    ok = ok && piv > 0.0 && isfinite(piv);
+    const double d = sqrt(piv);
+    a[k] = (lane == k) ? d : a[k] / d;  // lanes > k: L[lane][k]; lanes < k keep a finished row
+#pragma unroll
+    for (int j = k + 1; j < NX; ++j) {
+      const double ljk = __shfl_sync(DMPC_FULL_MASK, a[k], j);
+      if (lane >= j) a[j] = fma(-a[k], ljk, a[j]);
+    }
+  }
+  // X[i][c] = (delta_ic - sum_{k<i} L[i][k] X[k][c]) / L[i][i]; lane c keeps column c
+  double x[NX];
+#pragma unroll
+  for (int i = 0; i < NX; ++i) {
+    double acc = (lane == i) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < i; ++k) acc = fma(-__shfl_sync(DMPC_FULL_MASK, a[k], i), x[k], acc);
+    x[i] = acc / __shfl_sync(DMPC_FULL_MASK, a[i], i);
+  }
+  if (lane < NX) {
+#pragma unroll
+    for (int i = 0; i < NX; ++i) li[i * NX + lane] = x[i];
+  }
+  return ok;
+}

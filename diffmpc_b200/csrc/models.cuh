@@ -206,29 +206,30 @@ template <class T, int MODEL>
 __device__ void predict_next_state(int scheme, double dt, int nx, int nu, const T* x, const T* u,
                                    const T* p, T* xn) {
   constexpr int MX = ModelDims<MODEL>::NX;
+  // fixed-size models have nx == MX: compile-time trip counts keep the arrays in registers
   T k[MX], tmp[MX], acc[MX];
   StateDot<T, MODEL>::eval(nx, nu, x, u, p, k);
-  for (int i = 0; i < nx; ++i) xn[i] = x[i] + dt * k[i];
+  for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) xn[i] = x[i] + dt * k[i];
   if (scheme == DMPC_MIDPOINT) {
-    for (int i = 0; i < nx; ++i) tmp[i] = x[i] + 0.5 * dt * k[i];
+    for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) tmp[i] = x[i] + 0.5 * dt * k[i];
     StateDot<T, MODEL>::eval(nx, nu, tmp, u, p, acc);
-    for (int i = 0; i < nx; ++i) xn[i] = x[i] + dt * acc[i];
+    for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) xn[i] = x[i] + dt * acc[i];
   } else if (scheme == DMPC_RK4) {
-    for (int i = 0; i < nx; ++i) {
+    for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) {
       acc[i] = k[i];
       tmp[i] = x[i] + 0.5 * dt * k[i];
     }
     StateDot<T, MODEL>::eval(nx, nu, tmp, u, p, k);  // k2
-    for (int i = 0; i < nx; ++i) {
+    for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) {
       acc[i] = acc[i] + 2.0 * k[i];
       tmp[i] = x[i] + 0.5 * dt * k[i];
     }
     StateDot<T, MODEL>::eval(nx, nu, tmp, u, p, k);  // k3
-    for (int i = 0; i < nx; ++i) {
+    for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) {
       acc[i] = acc[i] + 2.0 * k[i];
       tmp[i] = x[i] + dt * k[i];
     }
     StateDot<T, MODEL>::eval(nx, nu, tmp, u, p, k);  // k4
-    for (int i = 0; i < nx; ++i) xn[i] = x[i] + ((1.0 / 6.0) * (acc[i] + k[i])) * dt;
+    for (int i = 0; i < (MODEL != DMPC_MODEL_LINEAR ? MX : nx); ++i) xn[i] = x[i] + ((1.0 / 6.0) * (acc[i] + k[i])) * dt;
   }
 }

@@ -256,7 +256,9 @@ __device__ void predict_next_state_linear(const Inst& s, const T* x, const T* u,
 template <int MODEL>
 __device__ __noinline__ void linearize_item(const Inst& s, const double* xb, const double* ub, int t, int d) {
   constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
-  const int nx = s.nx, nu = s.nu;
+  // fixed-size models have (nx, nu) == (MX, MU): compile-time trip counts keep the
+  // dual arrays in registers
+  const int nx = MODEL == DMPC_MODEL_LINEAR ? s.nx : MX, nu = MODEL == DMPC_MODEL_LINEAR ? s.nu : MU;
   Dual x[MX], u[MU], xn[MX];
   for (int j = 0; j < nx; ++j) x[j] = Dual(xb[t * nx + j], j == d ? 1.0 : 0.0);
   for (int j = 0; j < nu; ++j) u[j] = Dual(ub[t * nu + j], nx + j == d ? 1.0 : 0.0);
@@ -264,8 +266,9 @@ __device__ __noinline__ void linearize_item(const Inst& s, const double* xb, con
     // parameters as constants: read straight from memory to keep registers low
     predict_next_state_linear(s, x, u, xn);
   } else {
-    Dual p[12];
-    for (int k = 0; k < s.P && k < 12; ++k) p[k] = Dual(s.mp[k]);
+    Dual p[12];  // compile-time trip count keeps p in registers; unused slots are zero
+#pragma unroll
+    for (int k = 0; k < 12; ++k) p[k] = Dual(k < s.P ? s.mp[k] : 0.0);
     predict_next_state<Dual, MODEL>(s.scheme, s.dt, nx, nu, x, u, p, xn);
   }
   if (d < nx) {
@@ -362,6 +365,41 @@ __device__ void linearize_cost(const Inst& s, const double* xb, const double* ub
 // FP64 recurrence instead of the scaled FP32 iterations.
 __shared__ int sh_scaled_bad;
 
+// Li_t = L_t^-1 for every knot (theta_t = L_t L_t^T, FP64), one warp per block: in
+// registers for the nx with a row-pair PCG, else in the workspace (tmp as the
+// factorisation's working copy).  Sets sh_scaled_bad if a block has no factor.
+template <int NX>
+__device__ __noinline__ bool scaled_factors_regs(const Inst& s) {
+  constexpr int nn = NX * NX;
+  bool ok = true;
+  for (int t = threadIdx.x >> 5; t < s.K; t += blockDim.x >> 5)
+    ok = warp_chol_inverse_regs<NX>(s.th + (size_t)t * nn, s.li + (size_t)t * nn) && ok;
+  return ok;
+}
+
+__device__ void scaled_factors(const Inst& s) {
+  const int nx = s.nx, nn = nx * nx, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) sh_scaled_bad = 0;
+  __syncthreads();
+  bool ok = true;
+  switch (nx) {
+    case 3: ok = scaled_factors_regs<3>(s); break;
+    case 4: ok = scaled_factors_regs<4>(s); break;
+    case 6: ok = scaled_factors_regs<6>(s); break;
+    case 7: ok = scaled_factors_regs<7>(s); break;
+    case 12: ok = scaled_factors_regs<12>(s); break;
+    case 13: ok = scaled_factors_regs<13>(s); break;
+    default:
+      for (int t = threadIdx.x >> 5; t < s.K; t += blockDim.x >> 5) {
+        double* Lt = s.tmp + (size_t)t * nn;
+        for (int e = lane; e < nn; e += 32) Lt[e] = s.th[(size_t)t * nn + e];
+        __syncwarp();
+        ok = warp_chol_inverse(Lt, s.li + (size_t)t * nn, nx) && ok;
+      }
+  }
+  if (!ok && lane == 0) sh_scaled_bad = 1;
+}
+
 __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
   const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
   const int nn = nx * nx;
@@ -384,7 +422,7 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
       v = a + b + ((i == j) ? s.Qi[t * nx + i] : 0.0);
     }
     s.th[w] = v;
-    s.tmp[w] = v;
+    if (!fp32_copy) s.tmp[w] = v;  // working copy for the in-place Gauss-Jordan inverse
     if (t < N) {
       // phi_t = A_t D_t An_{t-1}^T : t == 0 -> A_0 D_0; t >= 1 -> -A_t D_t
       const double ph = s.A[((size_t)t * nx + i) * nx + j] * s.Qi[t * nx + j];
@@ -393,7 +431,20 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int t = warp; t < K; t += nwarp) warp_spd_inverse(s.tmp + (size_t)t * nn, s.ti + (size_t)t * nn, nx);
+  if (!fp32_copy) {
+    for (int t = warp; t < K; t += nwarp) warp_spd_inverse(s.tmp + (size_t)t * nn, s.ti + (size_t)t * nn, nx);
+  } else {
+    // Li_t = L_t^-1 with theta_t = L_t L_t^T, then theta_t^-1 = Li_t^T Li_t
+    scaled_factors(s);
+    __syncthreads();
+    for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
+      const int t = w / nn, e = w - t * nn, a = e / nx, b = e - a * nx;
+      const double* X = s.li + (size_t)t * nn;
+      double acc = 0.0;
+      for (int k = (a > b ? a : b); k < nx; ++k) acc += X[k * nx + a] * X[k * nx + b];
+      s.ti[w] = acc;
+    }
+  }
   __syncthreads();
   // T_t = theta_t^-1 phi_{t-1}  (t = 1..N), stored in tmp block t
   for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
@@ -417,20 +468,9 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
     s.pm[(size_t)k * nn + e] = -a;
   }
   if (fp32_copy) {
-    // scaled basis of the FP32 PCG: Li_t = L_t^-1 with theta_t = L_t L_t^T (FP64), then
-    // W_t = Li_t phi_{t-1} Li_{t-1}^T (t = 1..N) in FP32 at block t-1; block N is zero
+    // scaled basis of the FP32 PCG: W_t = Li_t phi_{t-1} Li_{t-1}^T (t = 1..N) in FP32 at
+    // block t-1; block N is zero
     __syncthreads();  // the P_t pass above has finished reading tmp
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) sh_scaled_bad = 0;
-    __syncthreads();
-    for (int t = warp; t < K; t += nwarp) {
-      double* Lt = s.tmp + (size_t)t * nn;
-      for (int e = lane; e < nn; e += 32) Lt[e] = s.th[(size_t)t * nn + e];
-      __syncwarp();
-      const bool ok = warp_chol_inverse(Lt, s.li + (size_t)t * nn, nx);
-      if (!ok && lane == 0) sh_scaled_bad = 1;
-    }
-    __syncthreads();
     // T_t = Li_t phi_{t-1} (t = 1..N) in tmp block t
     for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
       const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
@@ -1241,15 +1281,16 @@ template <int MODEL>
 __device__ __noinline__ double param_grad_item(const Inst& s, const double* xs, const double* us, const double* xt,
                                   const double* ut, const double* lstar, const double* ltil, int t, int k) {
   constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
-  const int nx = s.nx, nu = s.nu;
+  const int nx = MODEL == DMPC_MODEL_LINEAR ? s.nx : MX, nu = MODEL == DMPC_MODEL_LINEAR ? s.nu : MU;
   HDual x[MX], u[MU], f[MX];
   for (int j = 0; j < nx; ++j) x[j] = HDual(xs[t * nx + j], xt[t * nx + j], 0.0, 0.0);
   for (int j = 0; j < nu; ++j) u[j] = HDual(us[t * nu + j], ut[t * nu + j], 0.0, 0.0);
   if (MODEL == DMPC_MODEL_LINEAR) {
     predict_next_state_linear<HDual>(s, x, u, f, k);
   } else {
-    HDual p[12];
-    for (int q = 0; q < s.P && q < 12; ++q) p[q] = HDual(s.mp[q], 0.0, q == k ? 1.0 : 0.0, 0.0);
+    HDual p[12];  // compile-time trip count keeps p in registers; unused slots are zero
+#pragma unroll
+    for (int q = 0; q < 12; ++q) p[q] = HDual(q < s.P ? s.mp[q] : 0.0, 0.0, q == k ? 1.0 : 0.0, 0.0);
     predict_next_state<HDual, MODEL>(s.scheme, s.dt, nx, nu, x, u, p, f);
   }
   double acc = 0.0;
