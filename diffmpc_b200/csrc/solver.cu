@@ -400,8 +400,12 @@ __device__ void scaled_factors(const Inst& s) {
   if (!ok && lane == 0) sh_scaled_bad = 1;
 }
 
-__device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
-  const int nx = s.nx, nu = s.nu, N = s.N, K = s.K;
+// NXT > 0: compile-time nx, so every inner product is unrolled and its loads (of blocks
+// that live in L2) issue together; the triangular factors store exact zeros above the
+// diagonal, so those products run over the full range.
+template <int NXT>
+__device__ __noinline__ void assemble_schur_t(const Inst& s, bool fp32_copy) {
+  const int nx = NXT > 0 ? NXT : s.nx, nu = s.nu, N = s.N, K = s.K;
   const int nn = nx * nx;
   for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
     const int t = w / nn, e = w - t * nn, i = e / nx, j = e - i * nx;
@@ -417,6 +421,7 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
       const double* D = s.Qi + k * nx;
       const double* E = s.Ri + k * nu;
       double a = 0.0, b = 0.0;
+#pragma unroll
       for (int l = 0; l < nx; ++l) a += Ai[l] * D[l] * Aj[l];
       for (int l = 0; l < nu; ++l) b += Bi[l] * E[l] * Bj[l];
       v = a + b + ((i == j) ? s.Qi[t * nx + i] : 0.0);
@@ -441,7 +446,8 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
       const int t = w / nn, e = w - t * nn, a = e / nx, b = e - a * nx;
       const double* X = s.li + (size_t)t * nn;
       double acc = 0.0;
-      for (int k = (a > b ? a : b); k < nx; ++k) acc += X[k * nx + a] * X[k * nx + b];
+#pragma unroll
+      for (int k = 0; k < nx; ++k) acc += X[k * nx + a] * X[k * nx + b];  // X is zero above the diagonal
       s.ti[w] = acc;
     }
   }
@@ -453,6 +459,7 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
     const double* Ti = s.ti + (size_t)t * nn + i * nx;
     const double* Pk = s.ph + (size_t)k * nn + j;
     double a = 0.0;
+#pragma unroll
     for (int l = 0; l < nx; ++l) a += Ti[l] * Pk[l * nx];
     s.tmp[(size_t)t * nn + e] = a;
   }
@@ -464,6 +471,7 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
     const double* Tr = s.tmp + (size_t)t * nn + i * nx;
     const double* Tm = s.ti + (size_t)k * nn + j;
     double a = 0.0;
+#pragma unroll
     for (int l = 0; l < nx; ++l) a += Tr[l] * Tm[l * nx];
     s.pm[(size_t)k * nn + e] = -a;
   }
@@ -477,7 +485,8 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
       const double* Lr = s.li + (size_t)(k + 1) * nn + i * nx;
       const double* Pk = s.ph + (size_t)k * nn + j;
       double a = 0.0;
-      for (int l = 0; l <= i; ++l) a += Lr[l] * Pk[l * nx];
+#pragma unroll
+      for (int l = 0; l < nx; ++l) a += Lr[l] * Pk[l * nx];
       s.tmp[(size_t)(k + 1) * nn + e] = a;
     }
     __syncthreads();
@@ -490,13 +499,26 @@ __device__ __noinline__ void assemble_schur(const Inst& s, bool fp32_copy) {
         const double* Tr = s.tmp + (size_t)(k + 1) * nn + i * nx;
         const double* Lm = s.li + (size_t)k * nn + j * nx;  // (Li_{t-1}^T)[l][j] = Li_{t-1}[j][l]
         double a = 0.0;
-        for (int l = 0; l <= j; ++l) a += Tr[l] * Lm[l];
+#pragma unroll
+        for (int l = 0; l < nx; ++l) a += Tr[l] * Lm[l];
         v = (float)a;
       }
       s.w32[w] = v;
     }
   }
   __syncthreads();
+}
+
+__device__ void assemble_schur(const Inst& s, bool fp32_copy) {
+  switch (s.nx) {
+    case 3: assemble_schur_t<3>(s, fp32_copy); break;
+    case 4: assemble_schur_t<4>(s, fp32_copy); break;
+    case 6: assemble_schur_t<6>(s, fp32_copy); break;
+    case 7: assemble_schur_t<7>(s, fp32_copy); break;
+    case 12: assemble_schur_t<12>(s, fp32_copy); break;
+    case 13: assemble_schur_t<13>(s, fp32_copy); break;
+    default: assemble_schur_t<0>(s, fp32_copy);
+  }
 }
 
 // gamma = C + [Q0^-1 q0; A Q^-1 q + B R^-1 r + An Q_next^-1 q_next] (pcg.py:245-288),
