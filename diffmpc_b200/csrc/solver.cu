@@ -670,12 +670,13 @@ __device__ __noinline__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, d
 // FP32 refinement is not paying off: a refinement step cut eta64 by less than 1e4 (the
 // residual norm by less than 100x: kappa * eps32 is too close to 1 for the FP32 iterations
 // to reach their target in the true residual), or the FP32 iterations have used half of
-// the pcg.max_iter budget.  Finish the solve with the FP64 recurrence on the FP64 blocks
-// within the remaining budget, keeping the vectors in workspace regions that are free
-// during the PCG (t1, xn, C).
+// pcg.max_iter.  Finish the solve with the FP64 recurrence on the FP64 blocks, keeping the
+// vectors in workspace regions that are free during the PCG (t1, xn, C).  The recurrence
+// gets the full pcg.max_iter budget of the reference's loop: the FP32 iterations before it
+// are cheaper and restart at every refinement, so they are not charged against it, and a
+// QP's reported iteration count can reach 1.5 max_iter.
 __device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, double eps, double* red, int& par) {
-  const int left = max_iter - it > 1 ? max_iter - it : 1;
-  PcgOut o = pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, left, eps, red, par);
+  PcgOut o = pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, max_iter, eps, red, par);
   return PcgOut{it + o.it, o.eta};
 }
 constexpr double kStagnation = 1e-4;
