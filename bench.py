@@ -47,7 +47,7 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU-baseline sample")
     ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
-    ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress"],
+    ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress", "rollout"],
                     help="quadrotor = the headline; the others report the remaining workload shapes")
     return ap.parse_args()
 
@@ -462,6 +462,7 @@ def run_other_workload(args):
 
     from diffmpc_b200 import OptimalControlProblem, SQPSolver, workloads
     from diffmpc_b200.batch import solve_groups
+    from diffmpc_b200.sqp import SQPSolution
 
     dev = torch.device("cuda", 0)
     line = {"impl": "ours", "workload": args.workload, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -514,6 +515,50 @@ def run_other_workload(args):
                     pcg_iters_per_instance_p50=float(iters.quantile(0.5)),
                     pcg_iters_per_instance_p99=float(iters.quantile(0.99)),
                     status_success=int(sum(int((s.status == 0).sum()) for s in sols)))
+    elif args.workload == "rollout":
+        from diffmpc_b200.rollout import ClosedLoopRollout
+
+        B = args.batch if args.batch != 4096 else 1024
+        T = 50
+        dyn, st, bt, sp, (A, Bm, b) = workloads.rl_linear(B=B)
+        solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp, device=dev)
+        p = workloads.to_device(bt, dev)
+        Ad, Bd, bd = A.to(dev), Bm.to(dev), b.to(dev)
+        key = "weights_penalization_reference_state_trajectory"
+        roll = ClosedLoopRollout(solver, Ad, Bd, bd, T, warm_start=True)
+
+        def fused(grad):
+            w = {key: p[key].clone().requires_grad_(grad)}
+            c = roll(p["initial_state"], p, w)
+            if grad:
+                c.sum().backward()
+            return c
+
+        def host_loop():
+            w = {key: p[key].clone().requires_grad_(True)}
+            guess0 = solver.initial_guess(p)
+            guess, x, c = guess0, p["initial_state"], 0.0
+            for _ in range(T):
+                q = dict(p)
+                q["initial_state"] = x.detach()
+                sol = solver.solve(guess, q, w)
+                u = sol.controls[:, 0]
+                x = x @ Ad.T + u @ Bd.T + bd
+                c = c + (x ** 2).sum(-1) + (u ** 2).sum(-1)
+                guess = SQPSolution(*[v.detach() if isinstance(v, torch.Tensor) else v for v in sol])
+            c.sum().backward()
+            return c
+
+        ms_f, c_f = _timed(lambda: fused(False), args.steps, args.warmup)
+        ms_fb, c_fb = _timed(lambda: fused(True), args.steps, args.warmup)
+        ms_h, c_h = _timed(host_loop, args.steps, args.warmup)
+        line.update(metric="closed-loop MPC rollout, linear nx=8 nu=4 N=39, 50 steps, warm start, B=%d: "
+                           "MPC solves/s (B*steps per second), fwd+bwd through the rollout" % B,
+                    value=B * T / (ms_fb * 1e-3), ms_per_step=ms_fb, batch=B, sim_steps=T,
+                    fwd_only_solves_per_s=B * T / (ms_f * 1e-3), fwd_only_ms=ms_f,
+                    host_loop_solves_per_s=B * T / (ms_h * 1e-3), host_loop_ms=ms_h,
+                    max_rel_cost_diff_fused_vs_host_loop=float((c_fb - c_h).abs().max() / c_h.abs().max()),
+                    pcg_iters_per_solve=float(roll.last.pcg_hist.double().sum() / (B * T)))
     else:  # stress
         B = args.batch if args.batch != 4096 else 1024
         dyn, st, bt, sp = workloads.linear_stress(B=B)

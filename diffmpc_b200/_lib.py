@@ -39,6 +39,7 @@ EXPORTED_SYMBOLS = (
     "dmpc_kkt_recover",
     "dmpc_probe_fp32_fma",
     "dmpc_solve_fwd_noalloc",
+    "dmpc_rollout_fwd",
 )
 
 _p = ctypes.c_void_p
@@ -121,6 +122,29 @@ class Adjoint(ctypes.Structure):
     ]
 
 
+class Rollout(ctypes.Structure):
+    _fields_ = [
+        ("num_steps", _i32),
+        ("warm_start", _i32),
+        ("sim_A", _p),
+        ("sim_B", _p),
+        ("sim_b", _p),
+        ("step_initial_state", _p),
+        ("step_states", _p),
+        ("step_controls", _p),
+        ("step_dual", _p),
+        ("step_lin_states", _p),
+        ("step_lin_controls", _p),
+        ("step_status", _p),
+        ("step_num_iter", _p),
+        ("step_convergence_error", _p),
+        ("step_convergence_errors", _p),
+        ("step_linesearch_alphas", _p),
+        ("step_num_pcg_iters", _p),
+        ("running_cost", _p),
+    ]
+
+
 class DmpcError(RuntimeError):
     pass
 
@@ -175,6 +199,10 @@ def load():
     lib.dmpc_probe_fp32_fma.argtypes = [ctypes.c_int, ctypes.c_int, _p, _p]
     lib.dmpc_solve_fwd_noalloc.restype = ctypes.c_int
     lib.dmpc_solve_fwd_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(Group), ctypes.POINTER(SolverParams), _p]
+    lib.dmpc_rollout_fwd.restype = ctypes.c_int
+    lib.dmpc_rollout_fwd.argtypes = [
+        ctypes.POINTER(Group), ctypes.POINTER(Rollout), ctypes.POINTER(SolverParams), _p, ctypes.c_size_t, _p,
+    ]
     if lib.dmpc_abi_version() != 1:
         raise DmpcError("libdmpc.so ABI version mismatch")
     _lib = lib

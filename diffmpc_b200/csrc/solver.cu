@@ -139,8 +139,9 @@ struct Inst {
   float* w32;  // scaled-basis off-diagonal blocks W_t (FP32, row stride ld)
 };
 
-__device__ inline Inst make_inst(const DevGroup& G, int i, void* ws, float* smem_blocks) {
-  const dmpc_group& g = G.g;
+// g is the group's descriptor: G.g, or a view of it whose inputs/outputs point at one
+// step of a closed-loop rollout.
+__device__ inline Inst make_inst(const DevGroup& G, const dmpc_group& g, int i, void* ws, float* smem_blocks) {
   Inst s;
   s.model = g.model;
   s.nx = g.nx;
@@ -387,6 +388,7 @@ __device__ void scaled_factors(const Inst& s) {
     case 4: ok = scaled_factors_regs<4>(s); break;
     case 6: ok = scaled_factors_regs<6>(s); break;
     case 7: ok = scaled_factors_regs<7>(s); break;
+    case 8: ok = scaled_factors_regs<8>(s); break;
     case 12: ok = scaled_factors_regs<12>(s); break;
     case 13: ok = scaled_factors_regs<13>(s); break;
     default:
@@ -515,6 +517,7 @@ __device__ void assemble_schur(const Inst& s, bool fp32_copy) {
     case 4: assemble_schur_t<4>(s, fp32_copy); break;
     case 6: assemble_schur_t<6>(s, fp32_copy); break;
     case 7: assemble_schur_t<7>(s, fp32_copy); break;
+    case 8: assemble_schur_t<8>(s, fp32_copy); break;
     case 12: assemble_schur_t<12>(s, fp32_copy); break;
     case 13: assemble_schur_t<13>(s, fp32_copy); break;
     default: assemble_schur_t<0>(s, fp32_copy);
@@ -1204,6 +1207,7 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
       DMPC_PAIR(4)
       DMPC_PAIR(6)
       DMPC_PAIR(7)
+      DMPC_PAIR(8)
       DMPC_PAIR(12)
       DMPC_PAIR(13)
 #undef DMPC_PAIR
@@ -1215,16 +1219,14 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
 }
 
 // ---------------------------------------------------------------- forward kernel
-__global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevArgs args, void* ws) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  int gi, ii;
-  if (!locate(args, blockIdx.x, gi, ii)) return;
-  const DevGroup& G = args.grp[gi];
-  const dmpc_group& g = G.g;
-  const dmpc_solver_params& P = args.p;
+// The SQP loop of one instance (sqp.py:436-560): initial guess from g's states/controls/
+// dual, solution, status and histories back into g.  Called once per CTA by k_sqp_fwd and
+// once per simulation step by k_rollout_fwd.
+__device__ __forceinline__ void sqp_forward(const DevGroup& G, const dmpc_group& g, int ii,
+                                            const dmpc_solver_params& P, void* ws, unsigned char* smem) {
   SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
   __shared__ Inst sh_inst;  // per-instance context in shared memory: keeps ~70 pointer registers free
-  if (threadIdx.x == 0) sh_inst = make_inst(G, ii, ws, sv.blocks);
+  if (threadIdx.x == 0) sh_inst = make_inst(G, g, ii, ws, sv.blocks);
   __syncthreads();
   const Inst& s = sh_inst;
   const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K;
@@ -1297,6 +1299,101 @@ __global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevA
   }
 }
 
+__global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevArgs args, void* ws) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int gi, ii;
+  if (!locate(args, blockIdx.x, gi, ii)) return;
+  const DevGroup& G = args.grp[gi];
+  sqp_forward(G, G.g, ii, args.p, ws, smem);
+}
+
+// ---------------------------------------------------------------- closed-loop rollout
+// benchmark_diffmpc.py:140-175 (lax.scan of rollout_step, vmapped over instances), one CTA
+// per instance for all simulation steps: solve the MPC from x_k (warm-started from step
+// k-1's solution, or from the initial guess), apply u_k = controls[0], simulate
+// x_{k+1} = A x_k + B u_k + b and add |x_{k+1}|^2 + |u_k|^2 to the running cost.  Every
+// step's solution and last linearization point are kept for the adjoint sweep.
+__global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ DevArgs args,
+                                                        const __grid_constant__ dmpc_rollout ra, void* ws) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const DevGroup& G = args.grp[0];
+  const dmpc_group& g0 = G.g;
+  const int ii = blockIdx.x;
+  if (ii >= g0.batch) return;
+  const int nx = g0.nx, nu = g0.nu, Kmax = G.K, B = g0.batch;
+  const int mi = args.p.num_scp_iteration_max;
+  const size_t sx = (size_t)B * Kmax * nx, su = (size_t)B * Kmax * nu, sh = (size_t)B * mi;
+  const size_t ox = (size_t)ii * Kmax * nx, ou = (size_t)ii * Kmax * nu, oh = (size_t)ii * mi;
+  __shared__ dmpc_group sh_g;  // the group as seen by step k
+  __shared__ double sh_cost;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) ra.step_initial_state[(size_t)ii * nx + i] = g0.initial_state[(size_t)ii * nx + i];
+  if (threadIdx.x == 0) sh_cost = 0.0;
+  for (int k = 0; k < ra.num_steps; ++k) {
+    if (threadIdx.x == 0) {
+      dmpc_group v = g0;
+      v.initial_state = ra.step_initial_state + (size_t)k * B * nx;
+      v.states = ra.step_states + k * sx;
+      v.controls = ra.step_controls + k * su;
+      v.dual = ra.step_dual + k * sx;
+      v.lin_states = ra.step_lin_states + k * sx;
+      v.lin_controls = ra.step_lin_controls + k * su;
+      v.status = ra.step_status + (size_t)k * B;
+      v.num_iter = ra.step_num_iter + (size_t)k * B;
+      v.convergence_error = ra.step_convergence_error + (size_t)k * B;
+      v.convergence_errors = ra.step_convergence_errors + k * sh;
+      v.linesearch_alphas = ra.step_linesearch_alphas + k * sh;
+      v.num_pcg_iters = ra.step_num_pcg_iters + k * sh;
+      sh_g = v;
+    }
+    __syncthreads();
+    // guess of step k: step k-1's solution (warm start) or the initial guess; the SQP
+    // counter restarts either way (sqp.py:530-532)
+    const bool warm = ra.warm_start && k > 0;
+    const double* gsx = warm ? ra.step_states + (k - 1) * sx : g0.states;
+    const double* gsu = warm ? ra.step_controls + (k - 1) * su : g0.controls;
+    const double* gsl = warm ? ra.step_dual + (k - 1) * sx : g0.dual;
+    for (int w = threadIdx.x; w < Kmax * nx; w += blockDim.x) {
+      sh_g.states[ox + w] = gsx[ox + w];
+      sh_g.dual[ox + w] = gsl[ox + w];
+    }
+    for (int w = threadIdx.x; w < Kmax * nu; w += blockDim.x) sh_g.controls[ou + w] = gsu[ou + w];
+    const double* hce = warm ? ra.step_convergence_errors + (k - 1) * sh : g0.convergence_errors;
+    const double* hal = warm ? ra.step_linesearch_alphas + (k - 1) * sh : g0.linesearch_alphas;
+    const int32_t* hpc = warm ? ra.step_num_pcg_iters + (k - 1) * sh : g0.num_pcg_iters;
+    for (int w = threadIdx.x; w < mi; w += blockDim.x) {
+      sh_g.convergence_errors[oh + w] = hce[oh + w];
+      sh_g.linesearch_alphas[oh + w] = hal[oh + w];
+      sh_g.num_pcg_iters[oh + w] = hpc[oh + w];
+    }
+    if (threadIdx.x == 0)
+      sh_g.convergence_error[ii] = warm ? ra.step_convergence_error[(size_t)(k - 1) * B + ii] : g0.convergence_error[ii];
+    __syncthreads();
+    sqp_forward(G, sh_g, ii, args.p, ws, smem);
+    __syncthreads();
+    // simulator step and running cost (reward = -(|x_{k+1}|^2 + |u_k|^2))
+    const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
+    const double* u = sh_g.controls + ou;  // controls[0]
+    double* xn = ra.step_initial_state + ((size_t)(k + 1) * B + ii) * nx;
+    const double* A = ra.sim_A + (size_t)ii * nx * nx;
+    const double* Bm = ra.sim_B + (size_t)ii * nx * nu;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      double a = ra.sim_b[(size_t)ii * nx + i];
+      for (int j = 0; j < nx; ++j) a += A[i * nx + j] * x[j];
+      for (int j = 0; j < nu; ++j) a += Bm[i * nu + j] * u[j];
+      xn[i] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double c = 0.0;
+      for (int i = 0; i < nx; ++i) c += xn[i] * xn[i];
+      for (int j = 0; j < nu; ++j) c += u[j] * u[j];
+      sh_cost += c;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ra.running_cost[ii] = sh_cost;
+}
+
 // ---------------------------------------------------------------- adjoint kernel
 // Hyper-dual evaluation for model-parameter gradients: the e1e2 part of
 // lam*_{t+1} . F(z*_t + z~_t e1, theta + e_k e2) and the e2 part against lam~_{t+1}.
@@ -1331,7 +1428,7 @@ __global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevA
   const dmpc_solver_params& P = args.p;
   SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
   __shared__ Inst sh_inst;  // per-instance context in shared memory: keeps ~70 pointer registers free
-  if (threadIdx.x == 0) sh_inst = make_inst(G, ii, ws, sv.blocks);
+  if (threadIdx.x == 0) sh_inst = make_inst(G, g, ii, ws, sv.blocks);
   __syncthreads();
   const Inst& s = sh_inst;
   const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K, N = s.N;
@@ -1431,7 +1528,7 @@ __global__ void __launch_bounds__(256) k_linearize(const __grid_constant__ DevAr
   if (!locate(args, blockIdx.x, gi, ii)) return;
   const DevGroup& G = args.grp[gi];
   const dmpc_group& g = G.g;
-  Inst s = make_inst(G, ii, ws, nullptr);
+  Inst s = make_inst(G, g, ii, ws, nullptr);
   const int nx = s.nx, nu = s.nu, N = G.g.horizon, K = N + 1;
   const double* xb = g.states + (size_t)ii * K * nx;
   const double* ub = g.controls + (size_t)ii * K * nu;
@@ -1784,15 +1881,17 @@ int cuda_rc(cudaError_t e) {
   return DMPC_ERR_CUDA;
 }
 
-// Static shared memory of the SQP kernels: the per-instance context (sh_inst) and the
-// scaled-basis flag.  It counts against the same per-CTA opt-in limit as the dynamic
+// Static shared memory of the SQP kernels: the per-instance context (sh_inst), the
+// scaled-basis flag and, in k_rollout_fwd, the step view of the group.  It counts against the same per-CTA opt-in limit as the dynamic
 // request, so every dynamic size is checked against optin - kStaticSmemReserve.  A fixed
 // reserve (checked at compile time) keeps the size logic free of runtime queries.
 constexpr size_t kStaticSmemReserve = 1024;
-static_assert(sizeof(Inst) + 2 * sizeof(int) + 64 <= kStaticSmemReserve, "static shared memory reserve too small");
+// (k_rollout_fwd also keeps its per-step group view and running cost there)
+static_assert(sizeof(Inst) + sizeof(dmpc_group) + 2 * sizeof(double) + 64 <= kStaticSmemReserve,
+              "static shared memory reserve too small");
 
 // nx with a row-pair specialisation of the scaled FP32 PCG (pcg_pair_scaled)
-bool pair_nx(int nx) { return nx == 3 || nx == 4 || nx == 6 || nx == 7 || nx == 12 || nx == 13; }
+bool pair_nx(int nx) { return nx == 3 || nx == 4 || nx == 6 || nx == 7 || nx == 8 || nx == 12 || nx == 13; }
 
 // Threads per CTA (<= 512, the kernels' launch bound).  Mixed precision: one thread per
 // row pair when K * ceil(nx/2) fits, else one thread per row up to 512 threads (several
@@ -1989,6 +2088,35 @@ int dmpc_solve_adj(int n_groups, const dmpc_group* groups, const dmpc_adjoint* a
                    void* workspace, size_t workspace_bytes, void* stream) {
   if (!adj) return DMPC_ERR_INVALID;
   return launch_common(true, n_groups, groups, adj, params, workspace, workspace_bytes, stream);
+}
+
+int dmpc_rollout_fwd(const dmpc_group* group, const dmpc_rollout* ro, const dmpc_solver_params* params,
+                     void* workspace, size_t workspace_bytes, void* stream) {
+  if (!group || !ro || ro->num_steps < 1) return DMPC_ERR_INVALID;
+  if (!ro->sim_A || !ro->sim_B || !ro->sim_b || !ro->step_initial_state || !ro->step_states || !ro->step_controls ||
+      !ro->step_dual || !ro->step_lin_states || !ro->step_lin_controls || !ro->step_status || !ro->step_num_iter ||
+      !ro->step_convergence_error || !ro->step_convergence_errors || !ro->step_linesearch_alphas ||
+      !ro->step_num_pcg_iters || !ro->running_cost)
+    return DMPC_ERR_INVALID;
+  if (!group->initial_state || !group->states || !group->controls || !group->dual || !group->convergence_error ||
+      !group->convergence_errors || !group->linesearch_alphas || !group->num_pcg_iters)
+    return DMPC_ERR_INVALID;
+  DevArgs* args = new DevArgs;
+  size_t ws = 0, sm = 0;
+  int thr = 0;
+  int rc = fill_args(1, group, nullptr, params, args, &ws, &sm, &thr);
+  if (rc == DMPC_OK && (ws > workspace_bytes || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0))
+    rc = DMPC_ERR_WORKSPACE;
+  if (rc == DMPC_OK && args->total_blocks > 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_rollout_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) {
+      k_rollout_fwd<<<args->total_blocks, thr, sm, reinterpret_cast<cudaStream_t>(stream)>>>(*args, *ro, workspace);
+      e = cudaGetLastError();
+    }
+    rc = cuda_rc(e);
+  }
+  delete args;
+  return rc;
 }
 
 // Forward solve for callers that cannot allocate device memory: it uses the fixed

@@ -1,0 +1,168 @@
+"""Closed-loop MPC rollout fused on the device, differentiable w.r.t. the solver weights.
+
+The reference's reinforcement-learning benchmarks and notebooks run this loop
+(benchmarking/reinforcement-learning/benchmark_diffmpc.py:140-175): a ``lax.scan``
+over simulation steps whose body solves the MPC from the current state (warm-started
+from the previous solution), applies the first control, steps a discrete linear
+simulator ``x+ = A x + B u + b`` and accumulates ``|x+|^2 + |u|^2``; ``vmap`` runs it
+for a batch of initial states and ``jax.grad`` differentiates the summed cost w.r.t.
+the solver weights.
+
+Here one kernel launch (``dmpc_rollout_fwd``) runs every step of every instance: one
+CTA per instance keeps its workspace across the steps, so the loop pays no per-step
+launch or host round trip.  The backward pass is a reverse sweep with one batched
+``dmpc_solve_adj`` launch per step at that step's saved solution:
+
+    lam_T = 2 x_T
+    g_u,k = 2 u_k + B^T lam_{k+1}           (cotangent of controls[0] of step k)
+    grad_w += adjoint_k(dl/du_0 = g_u,k)
+    lam_k  = A^T lam_{k+1} + 2 x_k  (k >= 1)
+
+As in the reference, a solve's problem parameters (its initial state among them) are
+not differentiated (the custom VJP returns no cotangent for them, sqp.py:781-795), so
+the state reaches the gradient only through the simulator.  ``through_state=True``
+adds each solve's dL/dx_0 to lam_k, i.e. differentiates through the MPC's dependence on
+the state as well.
+"""
+
+from types import SimpleNamespace
+from typing import Dict, Optional
+
+import torch
+
+from . import _lib
+from .sqp import SQPSolution, SQPSolver, _Call, _ptr
+
+
+def _per_instance(m, B, shape, device):
+    t = torch.as_tensor(m, dtype=torch.float64, device=device)
+    if t.dim() == len(shape):
+        t = t.expand(B, *shape)
+    return t.reshape(B, *shape).contiguous()
+
+
+class _RolloutFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, roll, x0, problem_params, guess, keys, *vals):
+        solver = roll.solver
+        dev = x0.device
+        B = x0.shape[0]
+        params = dict(problem_params)
+        params.update({k: v.detach() for k, v in zip(keys, vals)})
+        params["initial_state"] = x0.detach()
+        if guess is None:
+            guess = solver.initial_guess(params)
+        call = _Call(solver, guess, params, B, dev)
+        nx, nu, K, T = call.nx, call.nu, call.K, roll.num_sim_steps
+        mi = solver.maxiter
+        f64 = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)  # noqa: E731
+        i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
+        st = SimpleNamespace(
+            A=_per_instance(roll.sim_A, B, (nx, nx), dev),
+            Bm=_per_instance(roll.sim_B, B, (nx, nu), dev),
+            b=_per_instance(roll.sim_b, B, (nx,), dev),
+            x=f64(T + 1, B, nx), states=f64(T, B, K, nx), controls=f64(T, B, K, nu), dual=f64(T, B, K, nx),
+            lin_states=f64(T, B, K, nx), lin_controls=f64(T, B, K, nu), status=i32(T, B), num_iter=i32(T, B),
+            conv=f64(T, B), conv_hist=f64(T, B, mi), alpha_hist=f64(T, B, mi), pcg_hist=i32(T, B, mi), cost=f64(B),
+        )
+        r = _lib.Rollout()
+        r.num_steps, r.warm_start = T, 1 if roll.warm_start else 0
+        r.sim_A, r.sim_B, r.sim_b = _ptr(st.A), _ptr(st.Bm), _ptr(st.b)
+        r.step_initial_state, r.step_states, r.step_controls = _ptr(st.x), _ptr(st.states), _ptr(st.controls)
+        r.step_dual, r.step_lin_states, r.step_lin_controls = _ptr(st.dual), _ptr(st.lin_states), _ptr(st.lin_controls)
+        r.step_status, r.step_num_iter, r.step_convergence_error = _ptr(st.status), _ptr(st.num_iter), _ptr(st.conv)
+        r.step_convergence_errors, r.step_linesearch_alphas = _ptr(st.conv_hist), _ptr(st.alpha_hist)
+        r.step_num_pcg_iters, r.running_cost = _ptr(st.pcg_hist), _ptr(st.cost)
+        lib = _lib.load()
+        n = lib.dmpc_workspace_size(1, call.group, solver._c_params)
+        if n == 0 and B > 0:
+            raise ValueError("invalid problem description for the B200 solver")
+        ws = solver._workspace(n, dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        ev = solver._event_pair()
+        _lib.check(lib.dmpc_rollout_fwd(call.group, r, solver._c_params, ws.data_ptr(), ws.numel(), stream),
+                   "dmpc_rollout_fwd")
+        solver._event_end(ev, "k_rollout_fwd")
+        roll.last = st
+        ctx.roll, ctx.call, ctx.st, ctx.keys = roll, call, st, keys
+        ctx.shapes = [v.shape for v in vals]
+        return st.cost.clone()
+
+    @staticmethod
+    def backward(ctx, g_cost):
+        roll, call, st, keys = ctx.roll, ctx.call, ctx.st, ctx.keys
+        solver = roll.solver
+        B, K, nx, nu, T = call.B, call.K, call.nx, call.nu, roll.num_sim_steps
+        go = g_cost.to(torch.float64).reshape(B, 1)
+        akeys = list(keys) + (["initial_state"] if roll.through_state and "initial_state" not in keys else [])
+        acc = {}
+        lam = 2.0 * go * st.x[T]
+        for k in reversed(range(T)):
+            u = st.controls[k, :, 0]
+            g_u = 2.0 * go * u + torch.einsum("bij,bi->bj", st.Bm, lam)
+            dlu = torch.zeros(B, K, nu, dtype=torch.float64, device=u.device)
+            dlu[:, 0] = g_u
+            g = _lib.Group.from_buffer_copy(call.group)
+            g.initial_state = _ptr(st.x[k])
+            g.states, g.controls, g.dual = _ptr(st.states[k]), _ptr(st.controls[k]), _ptr(st.dual[k])
+            g.lin_states, g.lin_controls = _ptr(st.lin_states[k]), _ptr(st.lin_controls[k])
+            g.status, g.num_iter, g.convergence_error = _ptr(st.status[k]), _ptr(st.num_iter[k]), _ptr(st.conv[k])
+            g.convergence_errors, g.linesearch_alphas = _ptr(st.conv_hist[k]), _ptr(st.alpha_hist[k])
+            g.num_pcg_iters = _ptr(st.pcg_hist[k])
+            view = SimpleNamespace(group=g, states=st.states[k], B=B, K=K, nx=nx, nu=nu)
+            dbg = torch.zeros(B, K, nx, dtype=torch.float64, device=u.device)
+            grads = solver._run_adj(view, None, dlu, dbg, akeys) if akeys else {}
+            for key in keys:
+                acc[key] = grads[key] if key not in acc else acc[key] + grads[key]
+            lam = torch.einsum("bij,bi->bj", st.A, lam)
+            if roll.through_state:
+                lam = lam + grads["initial_state"]
+            if k >= 1:
+                lam = lam + 2.0 * go * st.x[k]
+        out = []
+        for key, shape in zip(keys, ctx.shapes):
+            gk = acc[key].reshape(B, -1)
+            n = 1
+            for s in shape:
+                n *= s
+            out.append(gk.sum(0).reshape(shape) if gk.shape[1] == n else gk.reshape(shape))
+        return (None, lam, None, None, None) + tuple(out)
+
+
+class ClosedLoopRollout:
+    """MPC-in-the-loop rollout of ``num_sim_steps`` steps with the linear simulator
+    ``x+ = sim_A x + sim_B u + sim_b`` (each shared by the batch or given per instance).
+
+    ``rollout(initial_states, problem_params, weights)`` returns the running cost
+    ``sum_k |x_{k+1}|^2 + |u_k|^2`` per instance (shape ``(B,)``), differentiable with
+    respect to ``weights`` (any key ``SQPSolver.solve`` accepts) and ``initial_states``.
+    ``warm_start`` starts each solve from the previous step's solution, as the
+    reference's ``warm_start`` flag does.  After a call, ``last`` holds every step's
+    solution (``states``, ``controls``, ``x`` ...) and iteration counts.
+    """
+
+    def __init__(self, solver: SQPSolver, sim_A, sim_B, sim_b, num_sim_steps: int, warm_start: bool = True,
+                 through_state: bool = False):
+        if num_sim_steps < 1:
+            raise ValueError("num_sim_steps must be >= 1")
+        self.solver = solver
+        self.sim_A, self.sim_B, self.sim_b = sim_A, sim_B, sim_b
+        self.num_sim_steps = int(num_sim_steps)
+        self.warm_start = bool(warm_start)
+        self.through_state = bool(through_state)
+        self.last = None
+
+    def __call__(self, initial_states: torch.Tensor, problem_params: Dict, weights: Optional[Dict] = None,
+                 initial_guess: Optional[SQPSolution] = None) -> torch.Tensor:
+        weights = weights or {}
+        x0 = torch.as_tensor(initial_states, dtype=torch.float64)
+        keys = sorted(weights.keys())
+        vals = [torch.as_tensor(weights[k], dtype=torch.float64, device=x0.device) for k in keys]
+        return _RolloutFunction.apply(self, x0, problem_params, initial_guess, keys, *vals)
+
+    def solutions(self, k: int) -> SQPSolution:
+        """Step k's solution (no gradient)."""
+        st = self.last
+        return SQPSolution(st.states[k], st.controls[k], st.dual[k], None, None, None, st.status[k], st.num_iter[k],
+                           st.conv[k], st.conv_hist[k], st.alpha_hist[k], st.pcg_hist[k], None,
+                           st.lin_states[k], st.lin_controls[k])

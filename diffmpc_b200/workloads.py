@@ -104,6 +104,49 @@ def linear_stress(B=16384, seed=1004, nx=24, nu=8, N=128):
     return dyn, st, bt, sp
 
 
+def shrunk_stable_matrix(rng, nx, margin=1e-2):
+    """I + 0.1 N(0,1) with every eigenvalue of modulus >= 1 - margin divided by
+    (modulus + margin), so the spectrum lies strictly inside the unit circle
+    (benchmarking/reinforcement-learning/utils.py:34-48 describes this construction)."""
+    A = np.eye(nx) + 0.1 * rng.standard_normal((nx, nx))
+    lam, V = np.linalg.eig(A)
+    mod = np.abs(lam)
+    lam = np.where(mod < 1.0 - margin, lam, lam / (mod + margin))
+    return (V @ np.diag(lam) @ np.linalg.inv(V)).real
+
+
+def rl_linear(B=1024, seed=1005, nx=8, nu=4, N=39, warm_start=True):
+    """Closed-loop benchmark problem of the reference's reinforcement-learning scripts
+    (benchmark_diffmpc.py:40-100, utils.py): one stable discrete system shared by the batch
+    (A, B ~ N(0,1), b ~ 0.01 N(0,1)), x0 ~ 5 N(0,1), Q = I, R = I, no terminal weight, MPC
+    horizon N = 39 (40 knots) with dt = 1 Euler, so the MPC model's continuous-time A is
+    A - I; one SQP iteration with the line search at alpha = 1, PCG tolerance 1e-12.
+    Returns (dynamics, static params, batched params, solver params, (A, B, b))."""
+    rng = np.random.default_rng(seed)
+    A = shrunk_stable_matrix(rng, nx)
+    Bm = rng.standard_normal((nx, nu))
+    b = 0.01 * rng.standard_normal(nx)
+    x0 = 5.0 * rng.standard_normal((B, nx))
+    K = N + 1
+    tile = lambda a: np.repeat(a[None], B, axis=0)  # noqa: E731
+    batched = _base(
+        N, np.ones(B), 0, x0, np.zeros((B, nx)), np.zeros((B, K, nx)), np.zeros((B, K, nu)),
+        np.ones((B, nx)), np.ones((B, nu)), np.zeros((B, nx)), False,
+        {"A": tile(A - np.eye(nx)), "B": tile(Bm), "b": tile(b)},
+    )
+    dyn = LinearDynamics({
+        "num_states": nx, "num_controls": nu,
+        "names_states": [f"x{i}" for i in range(nx)], "names_controls": [f"u{i}" for i in range(nu)],
+    })
+    sp = load_solver_params("sqp.yaml")
+    sp["num_scp_iteration_max"] = 1
+    sp["pcg"]["tol_epsilon"] = 1e-12
+    sp["warm_start_backward"] = bool(warm_start)
+    sp["linesearch"] = True
+    sp["linesearch_alphas"] = [1.0]
+    return dyn, _static_of(batched), batched, sp, (_t(A), _t(Bm), _t(b))
+
+
 def attitude(B=1024, seed=1001, N=50):
     """Spacecraft attitude (quaternion + rate), random goal attitude."""
     rng = np.random.default_rng(seed)

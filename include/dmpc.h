@@ -161,6 +161,33 @@ typedef struct dmpc_adjoint {
   double* adj_controls;
 } dmpc_adjoint;
 
+/* Closed-loop rollout (benchmarking/reinforcement-learning/benchmark_diffmpc.py:140-175, the
+ * rollout_step scanned with lax.scan and vmapped over instances).  For k = 0..num_steps-1:
+ * solve the MPC with initial state x_k starting from step k-1's solution (warm_start) or from
+ * the group's initial guess, apply u_k = controls[0], simulate x_{k+1} = A x_k + B u_k + b and
+ * add |x_{k+1}|^2 + |u_k|^2 to the running cost.  All pointers are device memory; K = horizon+1,
+ * T = num_steps. */
+typedef struct {
+  int32_t num_steps;                /* T >= 1 */
+  int32_t warm_start;               /* 1: step k starts from step k-1's solution */
+  const double* sim_A;              /* (batch, nx, nx) discrete simulator */
+  const double* sim_B;              /* (batch, nx, nu) */
+  const double* sim_b;              /* (batch, nx) */
+  double* step_initial_state;       /* (T+1, batch, nx): x_0 (copied from the group) .. x_T */
+  double* step_states;              /* (T, batch, K, nx) solutions */
+  double* step_controls;            /* (T, batch, K, nu) */
+  double* step_dual;                /* (T, batch, K, nx) */
+  double* step_lin_states;          /* (T, batch, K, nx) last linearization points (adjoint) */
+  double* step_lin_controls;        /* (T, batch, K, nu) */
+  int32_t* step_status;             /* (T, batch) */
+  int32_t* step_num_iter;           /* (T, batch) */
+  double* step_convergence_error;   /* (T, batch) */
+  double* step_convergence_errors;  /* (T, batch, num_scp_iteration_max) */
+  double* step_linesearch_alphas;   /* (T, batch, num_scp_iteration_max) */
+  int32_t* step_num_pcg_iters;      /* (T, batch, num_scp_iteration_max) */
+  double* running_cost;             /* (batch) */
+} dmpc_rollout;
+
 int dmpc_abi_version(void);
 const char* dmpc_error_string(int code);
 /* Name of the last CUDA runtime error an entry point returned DMPC_ERR_CUDA for on the
@@ -242,6 +269,15 @@ int dmpc_compute_gamma(int batch, int N, int nx, int nu, const double* As_x_Qinv
                        const double* Asnext_x_Qinvnext, const double* Bs_x_Rinv, const double* Cs,
                        const double* Q0inv, const double* qvec, const double* rvec, double* gamma,
                        void* stream);
+
+/* The whole closed-loop rollout of every instance in ONE kernel launch (one CTA per
+ * instance runs all T steps); see dmpc_rollout.  `group` is a single group: its
+ * initial_state is x_0, and its states/controls/dual, convergence_error and histories hold
+ * the initial guess (read, not written).  Per-step solutions and linearization points go to
+ * the rollout's step arrays, so that the adjoint of step k is dmpc_solve_adj on a group
+ * view pointing at them.  Same workspace as dmpc_solve_fwd for `group`. */
+int dmpc_rollout_fwd(const dmpc_group* group, const dmpc_rollout* rollout, const dmpc_solver_params* params,
+                     void* workspace, size_t workspace_bytes, void* stream);
 
 /* get_states_controls_from_kkt_multipliers (pcg.py:290-348), general dense matrices:
  * lambda (batch,K,nx) -> states (batch,K,nx), controls (batch,K,nu) with row N zero. */

@@ -45,10 +45,11 @@ def test_struct_layout_matches_c(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "%s"\n'
-        "int main(){printf(\"%%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n\","
+        "int main(){printf(\"%%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n\","
         "sizeof(dmpc_solver_params),sizeof(dmpc_group),sizeof(dmpc_adjoint),"
         "offsetof(dmpc_solver_params,blocks_in_smem),offsetof(dmpc_group,lin_controls),"
-        "offsetof(dmpc_adjoint,param_grad_index),offsetof(dmpc_adjoint,adj_controls));}\n" % HEADER
+        "offsetof(dmpc_adjoint,param_grad_index),offsetof(dmpc_adjoint,adj_controls),"
+        "sizeof(dmpc_rollout),offsetof(dmpc_rollout,sim_A),offsetof(dmpc_rollout,running_cost));}\n" % HEADER
     )
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
@@ -57,6 +58,7 @@ def test_struct_layout_matches_c(tmp_path):
         ctypes.sizeof(_lib.SolverParams), ctypes.sizeof(_lib.Group), ctypes.sizeof(_lib.Adjoint),
         _lib.SolverParams.blocks_in_smem.offset, _lib.Group.lin_controls.offset,
         _lib.Adjoint.param_grad_index.offset, _lib.Adjoint.adj_controls.offset,
+        ctypes.sizeof(_lib.Rollout), _lib.Rollout.sim_A.offset, _lib.Rollout.running_cost.offset,
     ]
     assert got == want
 

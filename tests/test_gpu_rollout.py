@@ -1,0 +1,105 @@
+"""Fused closed-loop rollout (dmpc_rollout_fwd + a reverse sweep of dmpc_solve_adj).
+
+* Every step of the one-launch rollout equals the same step run as a separate
+  SQPSolver.solve call from the host (same kernels, same guess chain).
+* Running cost, per-step controls and gradients w.r.t. cost weights and the simulator's
+  model matrix match the oracle's rollout (oracle/rollout.py), whose gradient is pinned
+  to finite differences on the CPU: FP64 to 1e-9 / 1e-7, mixed precision at PCG tolerance
+  1e-13 to 1e-6 / 1e-5.
+"""
+
+import pytest
+import torch
+
+from diffmpc_b200 import OptimalControlProblem, SQPSolver, workloads
+from diffmpc_b200.rollout import ClosedLoopRollout
+from oracle.rollout import rollout as oracle_rollout
+from tests.oracle_util import oracle_solver, rel_err, tensor_params
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+KW = "weights_penalization_reference_state_trajectory"
+KU = "weights_penalization_control_squared"
+
+
+def _setup(precision, warm, B=3, N=12, seed=11):
+    dyn, st, bt, sp, (A, Bm, b) = workloads.rl_linear(B=B, seed=seed, nx=8, nu=4, N=N, warm_start=warm)
+    sp["precision"] = precision
+    sp["pcg"]["tol_epsilon"] = 1e-13
+    solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp)
+    return dyn, st, bt, sp, (A, Bm, b), solver, workloads.to_device(bt, DEV)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("warm", [True, False])
+def test_fused_rollout_steps_equal_host_loop_of_solves(precision, warm):
+    dyn, st, bt, sp, (A, Bm, b), solver, p = _setup(precision, warm)
+    T = 4
+    roll = ClosedLoopRollout(solver, A.to(DEV), Bm.to(DEV), b.to(DEV), T, warm_start=warm)
+    cost = roll(p["initial_state"], p)
+    torch.cuda.synchronize()
+    guess0 = solver.initial_guess(p)
+    guess, x = guess0, p["initial_state"]
+    c = torch.zeros_like(cost)
+    Ad, Bd, bd = A.to(DEV), Bm.to(DEV), b.to(DEV)
+    tol = 1e-10 if precision == "fp64" else 1e-5
+    for k in range(T):
+        q = dict(p)
+        q["initial_state"] = x
+        sol = solver.solve(guess, q)
+        assert rel_err(roll.last.controls[k], sol.controls) < tol, k
+        assert rel_err(roll.last.x[k], x) < tol, k
+        u = sol.controls[:, 0]
+        x = x @ Ad.T + u @ Bd.T + bd
+        c = c + (x ** 2).sum(-1) + (u ** 2).sum(-1)
+        guess = sol if warm else guess0
+    assert rel_err(cost, c) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("warm,through_state", [(True, False), (False, False), (True, True)])
+def test_rollout_cost_and_gradients_match_oracle(precision, warm, through_state):
+    dyn, st, bt, sp, (A, Bm, b), solver, p = _setup(precision, warm)
+    T = 3
+    wkeys = [KW, KU] + (["A"] if precision == "fp64" else [])
+    w = {k: p[k].clone().requires_grad_(True) for k in wkeys}
+    roll = ClosedLoopRollout(solver, A.to(DEV), Bm.to(DEV), b.to(DEV), T, warm_start=warm,
+                             through_state=through_state)
+    cost = roll(p["initial_state"], p, w)
+    cost.sum().backward()
+    torch.cuda.synchronize()
+
+    osolver = oracle_solver(dyn, st, sp)
+    op = tensor_params(bt)
+    ow = {k: op[k].clone().requires_grad_(True) for k in wkeys}
+    B = op["initial_state"].shape[0]
+    ocost, ous, _ = oracle_rollout(osolver, op, op["initial_state"], ow, A.expand(B, 8, 8), Bm.expand(B, 8, 4),
+                                   b.expand(B, 8), T, warm_start=warm, through_state=through_state)
+    ocost.sum().backward()
+    ctol, gtol = (1e-9, 1e-7) if precision == "fp64" else (1e-6, 1e-5)
+    assert rel_err(cost, ocost) < ctol
+    for k in range(T):
+        assert rel_err(roll.last.controls[k][:, 0], ous[k]) < ctol, k
+    for k in wkeys:
+        assert rel_err(w[k].grad, ow[k].grad) < gtol, k
+
+
+def test_reference_benchmark_configuration_matches_oracle():
+    """The reference's closed-loop benchmark configuration (nx=8, nu=4, 40 knots, one SQP
+    iteration with the line search at alpha = 1, PCG 1e-12, warm start), five steps."""
+    dyn, st, bt, sp, (A, Bm, b) = workloads.rl_linear(B=2, seed=5, N=39, warm_start=True)
+    solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp)
+    p = workloads.to_device(bt, DEV)
+    w = {KW: p[KW].clone().requires_grad_(True)}
+    roll = ClosedLoopRollout(solver, A.to(DEV), Bm.to(DEV), b.to(DEV), 5, warm_start=True)
+    cost = roll(p["initial_state"], p, w)
+    cost.sum().backward()
+    osolver = oracle_solver(dyn, st, sp)
+    op = tensor_params(bt)
+    ow = {KW: op[KW].clone().requires_grad_(True)}
+    ocost, _, _ = oracle_rollout(osolver, op, op["initial_state"], ow, A.expand(2, 8, 8), Bm.expand(2, 8, 4),
+                                 b.expand(2, 8), 5, warm_start=True)
+    ocost.sum().backward()
+    # mixed precision (the solver default) at the benchmark's PCG tolerance 1e-12
+    assert rel_err(cost, ocost) < 1e-6
+    assert rel_err(w[KW].grad, ow[KW].grad) < 1e-5
