@@ -518,7 +518,7 @@ def run_other_workload(args):
     elif args.workload == "rollout":
         from diffmpc_b200.rollout import ClosedLoopRollout
 
-        B = args.batch if args.batch != 4096 else 1024
+        B = args.batch if args.batch != 4096 else 64
         T = 50
         dyn, st, bt, sp, (A, Bm, b) = workloads.rl_linear(B=B)
         solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp, device=dev)
@@ -526,10 +526,11 @@ def run_other_workload(args):
         Ad, Bd, bd = A.to(dev), Bm.to(dev), b.to(dev)
         key = "weights_penalization_reference_state_trajectory"
         roll = ClosedLoopRollout(solver, Ad, Bd, bd, T, warm_start=True)
+        roll_cold = ClosedLoopRollout(solver, Ad, Bd, bd, T, warm_start=False)
 
-        def fused(grad):
+        def fused(grad, r=roll):
             w = {key: p[key].clone().requires_grad_(grad)}
-            c = roll(p["initial_state"], p, w)
+            c = r(p["initial_state"], p, w)
             if grad:
                 c.sum().backward()
             return c
@@ -552,11 +553,18 @@ def run_other_workload(args):
         ms_f, c_f = _timed(lambda: fused(False), args.steps, args.warmup)
         ms_fb, c_fb = _timed(lambda: fused(True), args.steps, args.warmup)
         ms_h, c_h = _timed(host_loop, args.steps, args.warmup)
+        ms_cold, _ = _timed(lambda: fused(True, roll_cold), args.steps, args.warmup)
         line.update(metric="closed-loop MPC rollout, linear nx=8 nu=4 N=39, 50 steps, warm start, B=%d: "
                            "MPC solves/s (B*steps per second), fwd+bwd through the rollout" % B,
                     value=B * T / (ms_fb * 1e-3), ms_per_step=ms_fb, batch=B, sim_steps=T,
                     fwd_only_solves_per_s=B * T / (ms_f * 1e-3), fwd_only_ms=ms_f,
                     host_loop_solves_per_s=B * T / (ms_h * 1e-3), host_loop_ms=ms_h,
+                    cold_start_solves_per_s=B * T / (ms_cold * 1e-3),
+                    reference_recorded={
+                        "fwd_solves_per_s": 23847, "fwd_bwd_solves_per_s": 14651,
+                        "config": "B=64, 40 knots, 50 steps, PCG 1e-12, warm start, FP64 JAX on an unrecorded GPU",
+                        "source": "benchmarking/reinforcement-learning/timing_results/"
+                                  "timing_64_40_12_pcg=1e-12_warmstart=True/diffmpc_cuda:0_{fwd,bwd}.npy (median of 100)"},
                     max_rel_cost_diff_fused_vs_host_loop=float((c_fb - c_h).abs().max() / c_h.abs().max()),
                     pcg_iters_per_solve=float(roll.last.pcg_hist.double().sum() / (B * T)))
     else:  # stress

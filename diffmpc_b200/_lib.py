@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "dmpc_probe_fp32_fma",
     "dmpc_solve_fwd_noalloc",
     "dmpc_rollout_fwd",
+    "dmpc_rollout_adj",
 )
 
 _p = ctypes.c_void_p
@@ -145,6 +146,16 @@ class Rollout(ctypes.Structure):
     ]
 
 
+class RolloutAdjoint(ctypes.Structure):
+    _fields_ = [
+        ("cost_cotangent", _p),
+        ("through_state", _i32),
+        ("scratch_dl_dcontrols", _p),
+        ("scratch_dual", _p),
+        ("g_initial_state", _p),
+    ]
+
+
 class DmpcError(RuntimeError):
     pass
 
@@ -202,6 +213,11 @@ def load():
     lib.dmpc_rollout_fwd.restype = ctypes.c_int
     lib.dmpc_rollout_fwd.argtypes = [
         ctypes.POINTER(Group), ctypes.POINTER(Rollout), ctypes.POINTER(SolverParams), _p, ctypes.c_size_t, _p,
+    ]
+    lib.dmpc_rollout_adj.restype = ctypes.c_int
+    lib.dmpc_rollout_adj.argtypes = [
+        ctypes.POINTER(Group), ctypes.POINTER(Rollout), ctypes.POINTER(Adjoint), ctypes.POINTER(RolloutAdjoint),
+        ctypes.POINTER(SolverParams), _p, ctypes.c_size_t, _p,
     ]
     if lib.dmpc_abi_version() != 1:
         raise DmpcError("libdmpc.so ABI version mismatch")

@@ -1308,6 +1308,27 @@ __global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevA
 }
 
 // ---------------------------------------------------------------- closed-loop rollout
+// The group as seen by simulation step k: initial state x_k, and solution, linearization
+// point, status and histories in step k's slices of the rollout arrays.
+__device__ inline dmpc_group rollout_step_view(const dmpc_group& g0, const dmpc_rollout& ra, int k, int Kmax, int mi) {
+  const size_t B = g0.batch;
+  const size_t sx = B * Kmax * g0.nx, su = B * Kmax * g0.nu, sh = B * mi;
+  dmpc_group v = g0;
+  v.initial_state = ra.step_initial_state + (size_t)k * B * g0.nx;
+  v.states = ra.step_states + k * sx;
+  v.controls = ra.step_controls + k * su;
+  v.dual = ra.step_dual + k * sx;
+  v.lin_states = ra.step_lin_states + k * sx;
+  v.lin_controls = ra.step_lin_controls + k * su;
+  v.status = ra.step_status + (size_t)k * B;
+  v.num_iter = ra.step_num_iter + (size_t)k * B;
+  v.convergence_error = ra.step_convergence_error + (size_t)k * B;
+  v.convergence_errors = ra.step_convergence_errors + k * sh;
+  v.linesearch_alphas = ra.step_linesearch_alphas + k * sh;
+  v.num_pcg_iters = ra.step_num_pcg_iters + k * sh;
+  return v;
+}
+
 // benchmark_diffmpc.py:140-175 (lax.scan of rollout_step, vmapped over instances), one CTA
 // per instance for all simulation steps: solve the MPC from x_k (warm-started from step
 // k-1's solution, or from the initial guess), apply u_k = controls[0], simulate
@@ -1329,22 +1350,7 @@ __global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ 
   for (int i = threadIdx.x; i < nx; i += blockDim.x) ra.step_initial_state[(size_t)ii * nx + i] = g0.initial_state[(size_t)ii * nx + i];
   if (threadIdx.x == 0) sh_cost = 0.0;
   for (int k = 0; k < ra.num_steps; ++k) {
-    if (threadIdx.x == 0) {
-      dmpc_group v = g0;
-      v.initial_state = ra.step_initial_state + (size_t)k * B * nx;
-      v.states = ra.step_states + k * sx;
-      v.controls = ra.step_controls + k * su;
-      v.dual = ra.step_dual + k * sx;
-      v.lin_states = ra.step_lin_states + k * sx;
-      v.lin_controls = ra.step_lin_controls + k * su;
-      v.status = ra.step_status + (size_t)k * B;
-      v.num_iter = ra.step_num_iter + (size_t)k * B;
-      v.convergence_error = ra.step_convergence_error + (size_t)k * B;
-      v.convergence_errors = ra.step_convergence_errors + k * sh;
-      v.linesearch_alphas = ra.step_linesearch_alphas + k * sh;
-      v.num_pcg_iters = ra.step_num_pcg_iters + k * sh;
-      sh_g = v;
-    }
+    if (threadIdx.x == 0) sh_g = rollout_step_view(g0, ra, k, Kmax, mi);
     __syncthreads();
     // guess of step k: step k-1's solution (warm start) or the initial guess; the SQP
     // counter restarts either way (sqp.py:530-532)
@@ -1418,14 +1424,11 @@ __device__ __noinline__ double param_grad_item(const Inst& s, const double* xs, 
   return acc;
 }
 
-__global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevArgs args, void* ws) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  int gi, ii;
-  if (!locate(args, blockIdx.x, gi, ii)) return;
-  const DevGroup& G = args.grp[gi];
-  const dmpc_group& g = G.g;
-  const dmpc_adjoint& a = G.a;
-  const dmpc_solver_params& P = args.p;
+// The adjoint of one instance's solve (sqp.py:668-798) at the linearization point saved in
+// g.  With `acc`, the parameter gradients are added to the outputs (the rollout's sweep
+// over its steps) instead of stored; a null dl_dstates stands for zeros.
+__device__ __forceinline__ void sqp_adjoint(const DevGroup& G, const dmpc_group& g, const dmpc_adjoint& a, int ii,
+                                            const dmpc_solver_params& P, void* ws, unsigned char* smem, bool acc) {
   SmemView sv = carve_smem(smem, g.nx, G.K, P.precision);
   __shared__ Inst sh_inst;  // per-instance context in shared memory: keeps ~70 pointer registers free
   if (threadIdx.x == 0) sh_inst = make_inst(G, g, ii, ws, sv.blocks);
@@ -1441,7 +1444,7 @@ __global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevA
   linearize_dynamics(s, s.xb, s.ub);
   linearize_cost(s, s.xb, s.ub);
   // q = -dl/dx, r = -dl/du[:-1] (sqp.py:682-683)
-  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.q[w] = -a.dl_dstates[ox + w];
+  for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.q[w] = a.dl_dstates ? -a.dl_dstates[ox + w] : -0.0;
   for (int w = threadIdx.x; w < N * nu; w += blockDim.x) s.r[w] = -a.dl_dcontrols[ou + w];
   __syncthreads();
   assemble_schur(s, P.precision != DMPC_PREC_FP64);
@@ -1473,26 +1476,28 @@ __global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevA
     const double dN = xs[N * nx + j] - s.xf[j];
     const double xtN = xt[N * nx + j];
     gwx += 2.0 * dN * xtN;
-    if (a.g_w_x) a.g_w_x[(size_t)ii * nx + j] = -gwx;
-    if (a.g_w_f) a.g_w_f[(size_t)ii * nx + j] = -2.0 * dN * xtN;
-    if (a.g_initial_state) a.g_initial_state[(size_t)ii * nx + j] = s.lam[j];
-    if (a.g_final_state) a.g_final_state[(size_t)ii * nx + j] = 2.0 * (s.wx[j] + s.wf[j]) * xtN;
+    const size_t o = (size_t)ii * nx + j;
+    if (a.g_w_x) a.g_w_x[o] = (acc ? a.g_w_x[o] : 0.0) - gwx;
+    if (a.g_w_f) a.g_w_f[o] = (acc ? a.g_w_f[o] : 0.0) - 2.0 * dN * xtN;
+    if (a.g_initial_state) a.g_initial_state[o] = (acc ? a.g_initial_state[o] : 0.0) + s.lam[j];
+    if (a.g_final_state) a.g_final_state[o] = (acc ? a.g_final_state[o] : 0.0) + 2.0 * (s.wx[j] + s.wf[j]) * xtN;
   } else if (j < nx + nu) {
     const int k = j - nx;
     double gwu = 0.0;
     for (int t = 0; t < N; ++t)
       gwu += 2.0 * (us[t * nu + k] - (s.pen ? s.uref[t * nu + k] : 0.0)) * ut[t * nu + k];
-    if (a.g_w_u) a.g_w_u[(size_t)ii * nu + k] = -gwu;
+    const size_t o = (size_t)ii * nu + k;
+    if (a.g_w_u) a.g_w_u[o] = (acc ? a.g_w_u[o] : 0.0) - gwu;
   }
   if (a.g_reference_state)
     for (int w = threadIdx.x; w < Kmax * nx; w += blockDim.x) {
       const int t = w / nx, i = w - t * nx;
-      a.g_reference_state[ox + w] = (t < N) ? 2.0 * s.wx[i] * xt[w] : 0.0;
+      a.g_reference_state[ox + w] = (acc ? a.g_reference_state[ox + w] : 0.0) + ((t < N) ? 2.0 * s.wx[i] * xt[w] : 0.0);
     }
   if (a.g_reference_control)
     for (int w = threadIdx.x; w < Kmax * nu; w += blockDim.x) {
       const int t = w / nu, i = w - t * nu;
-      a.g_reference_control[ou + w] = (t < N && s.pen) ? 2.0 * s.wu[i] * ut[w] : 0.0;
+      a.g_reference_control[ou + w] = (acc ? a.g_reference_control[ou + w] : 0.0) + ((t < N && s.pen) ? 2.0 * s.wu[i] * ut[w] : 0.0);
     }
   // model parameters: hyper-dual mixed partials through the integrator
   const int ng = a.n_param_grads;
@@ -1512,11 +1517,86 @@ __global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevA
     }
     __syncthreads();
     for (int q = threadIdx.x; q < ng; q += blockDim.x) {
-      double acc = 0.0;
-      for (int t = 0; t < N; ++t) acc += s.contrib[(size_t)q * K + t];
-      a.g_model_params[(size_t)ii * ng + q] = -acc;
+      double sum = 0.0;
+      for (int t = 0; t < N; ++t) sum += s.contrib[(size_t)q * K + t];
+      a.g_model_params[(size_t)ii * ng + q] = (acc ? a.g_model_params[(size_t)ii * ng + q] : 0.0) - sum;
     }
   }
+}
+
+__global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevArgs args, void* ws) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int gi, ii;
+  if (!locate(args, blockIdx.x, gi, ii)) return;
+  const DevGroup& G = args.grp[gi];
+  sqp_adjoint(G, G.g, G.a, ii, args.p, ws, smem, false);
+}
+
+// Reverse sweep of the rollout's gradient (what jax.grad of the reference's scan computes):
+// with lam_T = 2 c x_T (c = dL/d running cost), for k = T-1 .. 0
+//   dl/du_0 of step k  = 2 c u_k + B^T lam_{k+1}
+//   adjoint of step k's solve, parameter gradients accumulated into adj's outputs
+//   lam_k = A^T lam_{k+1} + 2 c x_k (k >= 1) [+ the solve's dL/dx_0 if through_state]
+// and dL/dx_0 = lam_0.  One CTA per instance, all steps in one launch.
+__global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ DevArgs args,
+                                                        const __grid_constant__ dmpc_rollout ra,
+                                                        const __grid_constant__ dmpc_rollout_adjoint rr, void* ws) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const DevGroup& G = args.grp[0];
+  const dmpc_group& g0 = G.g;
+  const int ii = blockIdx.x;
+  if (ii >= g0.batch) return;
+  const int nx = g0.nx, nu = g0.nu, Kmax = G.K, B = g0.batch;
+  const int mi = args.p.num_scp_iteration_max;
+  const size_t ox = (size_t)ii * Kmax * nx, ou = (size_t)ii * Kmax * nu;
+  __shared__ dmpc_group sh_g;
+  __shared__ dmpc_adjoint sh_a;
+  __shared__ double sh_lam[DMPC_MAX_NX], sh_nxt[DMPC_MAX_NX];
+  const double c = rr.cost_cotangent[ii];
+  const int T = ra.num_steps;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = 2.0 * c * ra.step_initial_state[((size_t)T * B + ii) * nx + i];
+  for (int w = threadIdx.x; w < Kmax * nu; w += blockDim.x) rr.scratch_dl_dcontrols[ou + w] = 0.0;
+  __syncthreads();
+  for (int k = T - 1; k >= 0; --k) {
+    if (threadIdx.x == 0) {
+      sh_g = rollout_step_view(g0, ra, k, Kmax, mi);
+      dmpc_adjoint a = G.a;
+      a.dl_dstates = nullptr;
+      a.dl_dcontrols = rr.scratch_dl_dcontrols;
+      a.dual_backward_guess = nullptr;  // the carried solution's backward guess is zero
+      a.dual_backward = rr.scratch_dual;
+      a.num_pcg_iter = nullptr;
+      a.g_initial_state = nullptr;
+      a.adj_states = nullptr;
+      a.adj_controls = nullptr;
+      sh_a = a;
+    }
+    __syncthreads();
+    const double* u = sh_g.controls + ou;  // u_k = controls[0]
+    const double* Bm = ra.sim_B + (size_t)ii * nx * nu;
+    for (int j = threadIdx.x; j < nu; j += blockDim.x) {
+      double v = 2.0 * c * u[j];
+      for (int i = 0; i < nx; ++i) v += Bm[i * nu + j] * sh_lam[i];
+      rr.scratch_dl_dcontrols[ou + j] = v;
+    }
+    __syncthreads();
+    sqp_adjoint(G, sh_g, sh_a, ii, args.p, ws, smem, true);
+    __syncthreads();
+    const double* A = ra.sim_A + (size_t)ii * nx * nx;
+    const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      double v = 0.0;
+      for (int j = 0; j < nx; ++j) v += A[j * nx + i] * sh_lam[j];
+      if (rr.through_state) v += rr.scratch_dual[ox + i];  // the solve's dL/dx_0 = lam~_0
+      if (k >= 1) v += 2.0 * c * x[i];
+      sh_nxt[i] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = sh_nxt[i];
+    __syncthreads();
+  }
+  if (rr.g_initial_state)
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) rr.g_initial_state[(size_t)ii * nx + i] = sh_lam[i];
 }
 
 // ---------------------------------------------------------------- dense-layout parity kernels
@@ -1882,12 +1962,14 @@ int cuda_rc(cudaError_t e) {
 }
 
 // Static shared memory of the SQP kernels: the per-instance context (sh_inst), the
-// scaled-basis flag and, in k_rollout_fwd, the step view of the group.  It counts against the same per-CTA opt-in limit as the dynamic
+// scaled-basis flag and, in the rollout kernels, the step views and the state cotangent.  It counts against the same per-CTA opt-in limit as the dynamic
 // request, so every dynamic size is checked against optin - kStaticSmemReserve.  A fixed
 // reserve (checked at compile time) keeps the size logic free of runtime queries.
-constexpr size_t kStaticSmemReserve = 1024;
-// (k_rollout_fwd also keeps its per-step group view and running cost there)
-static_assert(sizeof(Inst) + sizeof(dmpc_group) + 2 * sizeof(double) + 64 <= kStaticSmemReserve,
+constexpr size_t kStaticSmemReserve = 2048;
+// (the rollout kernels also keep the per-step group and adjoint views and the state
+// cotangent there)
+static_assert(sizeof(Inst) + sizeof(dmpc_group) + sizeof(dmpc_adjoint) + 2 * DMPC_MAX_NX * sizeof(double) +
+                      2 * sizeof(double) + 64 <= kStaticSmemReserve,
               "static shared memory reserve too small");
 
 // nx with a row-pair specialisation of the scaled FP32 PCG (pcg_pair_scaled)
@@ -2088,6 +2170,33 @@ int dmpc_solve_adj(int n_groups, const dmpc_group* groups, const dmpc_adjoint* a
                    void* workspace, size_t workspace_bytes, void* stream) {
   if (!adj) return DMPC_ERR_INVALID;
   return launch_common(true, n_groups, groups, adj, params, workspace, workspace_bytes, stream);
+}
+
+int dmpc_rollout_adj(const dmpc_group* group, const dmpc_rollout* ro, const dmpc_adjoint* adj,
+                     const dmpc_rollout_adjoint* rr, const dmpc_solver_params* params, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+  if (!group || !ro || !adj || !rr || ro->num_steps < 1) return DMPC_ERR_INVALID;
+  if (!ro->sim_A || !ro->sim_B || !ro->step_initial_state || !ro->step_states || !ro->step_controls ||
+      !ro->step_dual || !ro->step_lin_states || !ro->step_lin_controls || !ro->step_status || !ro->step_num_iter ||
+      !ro->step_convergence_error || !ro->step_convergence_errors || !ro->step_linesearch_alphas ||
+      !ro->step_num_pcg_iters || !rr->cost_cotangent || !rr->scratch_dl_dcontrols || !rr->scratch_dual)
+    return DMPC_ERR_INVALID;
+  DevArgs* args = new DevArgs;
+  size_t ws = 0, sm = 0;
+  int thr = 0;
+  int rc = fill_args(1, group, adj, params, args, &ws, &sm, &thr);
+  if (rc == DMPC_OK && (ws > workspace_bytes || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0))
+    rc = DMPC_ERR_WORKSPACE;
+  if (rc == DMPC_OK && args->total_blocks > 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_rollout_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) {
+      k_rollout_adj<<<args->total_blocks, thr, sm, reinterpret_cast<cudaStream_t>(stream)>>>(*args, *ro, *rr, workspace);
+      e = cudaGetLastError();
+    }
+    rc = cuda_rc(e);
+  }
+  delete args;
+  return rc;
 }
 
 int dmpc_rollout_fwd(const dmpc_group* group, const dmpc_rollout* ro, const dmpc_solver_params* params,

@@ -10,8 +10,9 @@ the solver weights.
 
 Here one kernel launch (``dmpc_rollout_fwd``) runs every step of every instance: one
 CTA per instance keeps its workspace across the steps, so the loop pays no per-step
-launch or host round trip.  The backward pass is a reverse sweep with one batched
-``dmpc_solve_adj`` launch per step at that step's saved solution:
+launch or host round trip.  The backward pass (``dmpc_rollout_adj``, also one launch)
+sweeps the steps in reverse and runs the adjoint of each step's solve at its saved
+solution:
 
     lam_T = 2 x_T
     g_u,k = 2 u_k + B^T lam_{k+1}           (cotangent of controls[0] of step k)
@@ -31,7 +32,7 @@ from typing import Dict, Optional
 import torch
 
 from . import _lib
-from .sqp import SQPSolution, SQPSolver, _Call, _ptr
+from .sqp import AdjointSpec, SQPSolution, SQPSolver, _Call, _ptr
 
 
 def _per_instance(m, B, shape, device):
@@ -84,41 +85,18 @@ class _RolloutFunction(torch.autograd.Function):
                    "dmpc_rollout_fwd")
         solver._event_end(ev, "k_rollout_fwd")
         roll.last = st
-        ctx.roll, ctx.call, ctx.st, ctx.keys = roll, call, st, keys
+        ctx.roll, ctx.call, ctx.st, ctx.keys, ctx.r = roll, call, st, keys, r
         ctx.shapes = [v.shape for v in vals]
         return st.cost.clone()
 
     @staticmethod
     def backward(ctx, g_cost):
         roll, call, st, keys = ctx.roll, ctx.call, ctx.st, ctx.keys
-        solver = roll.solver
-        B, K, nx, nu, T = call.B, call.K, call.nx, call.nu, roll.num_sim_steps
-        go = g_cost.to(torch.float64).reshape(B, 1)
-        akeys = list(keys) + (["initial_state"] if roll.through_state and "initial_state" not in keys else [])
-        acc = {}
-        lam = 2.0 * go * st.x[T]
-        for k in reversed(range(T)):
-            u = st.controls[k, :, 0]
-            g_u = 2.0 * go * u + torch.einsum("bij,bi->bj", st.Bm, lam)
-            dlu = torch.zeros(B, K, nu, dtype=torch.float64, device=u.device)
-            dlu[:, 0] = g_u
-            g = _lib.Group.from_buffer_copy(call.group)
-            g.initial_state = _ptr(st.x[k])
-            g.states, g.controls, g.dual = _ptr(st.states[k]), _ptr(st.controls[k]), _ptr(st.dual[k])
-            g.lin_states, g.lin_controls = _ptr(st.lin_states[k]), _ptr(st.lin_controls[k])
-            g.status, g.num_iter, g.convergence_error = _ptr(st.status[k]), _ptr(st.num_iter[k]), _ptr(st.conv[k])
-            g.convergence_errors, g.linesearch_alphas = _ptr(st.conv_hist[k]), _ptr(st.alpha_hist[k])
-            g.num_pcg_iters = _ptr(st.pcg_hist[k])
-            view = SimpleNamespace(group=g, states=st.states[k], B=B, K=K, nx=nx, nu=nu)
-            dbg = torch.zeros(B, K, nx, dtype=torch.float64, device=u.device)
-            grads = solver._run_adj(view, None, dlu, dbg, akeys) if akeys else {}
-            for key in keys:
-                acc[key] = grads[key] if key not in acc else acc[key] + grads[key]
-            lam = torch.einsum("bij,bi->bj", st.A, lam)
-            if roll.through_state:
-                lam = lam + grads["initial_state"]
-            if k >= 1:
-                lam = lam + 2.0 * go * st.x[k]
+        if roll.fused_backward:
+            acc, gx0 = _fused_sweep(ctx, g_cost)
+        else:
+            acc, gx0 = _per_step_sweep(ctx, g_cost)
+        B = call.B
         out = []
         for key, shape in zip(keys, ctx.shapes):
             gk = acc[key].reshape(B, -1)
@@ -126,7 +104,69 @@ class _RolloutFunction(torch.autograd.Function):
             for s in shape:
                 n *= s
             out.append(gk.sum(0).reshape(shape) if gk.shape[1] == n else gk.reshape(shape))
-        return (None, lam, None, None, None) + tuple(out)
+        return (None, gx0, None, None, None) + tuple(out)
+
+
+def _fused_sweep(ctx, g_cost):
+    """dmpc_rollout_adj: the whole reverse sweep in one launch per parameter chunk."""
+    roll, call, st, keys = ctx.roll, ctx.call, ctx.st, ctx.keys
+    solver = roll.solver
+    B, K, nx, nu = call.B, call.K, call.nx, call.nu
+    dev = st.x.device
+    go = g_cost.to(torch.float64).reshape(B).contiguous()
+    view = SimpleNamespace(group=call.group, states=st.states[0], B=B, K=K, nx=nx, nu=nu)
+    spec = AdjointSpec(solver.program.dynamics, view, None, None, None, keys)
+    scratch_u = torch.zeros(B, K, nu, dtype=torch.float64, device=dev)
+    scratch_l = torch.zeros(B, K, nx, dtype=torch.float64, device=dev)
+    gx0 = torch.zeros(B, nx, dtype=torch.float64, device=dev)
+    rr = _lib.RolloutAdjoint()
+    rr.cost_cotangent, rr.through_state = _ptr(go), 1 if roll.through_state else 0
+    rr.scratch_dl_dcontrols, rr.scratch_dual, rr.g_initial_state = _ptr(scratch_u), _ptr(scratch_l), _ptr(gx0)
+    lib = _lib.load()
+    ws = solver._workspace(lib.dmpc_workspace_size(1, call.group, solver._c_params), dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for ci in range(spec.n_chunks):
+        spec.select_chunk(ci)
+        ev = solver._event_pair()
+        _lib.check(lib.dmpc_rollout_adj(call.group, ctx.r, spec.adj, rr, solver._c_params, ws.data_ptr(), ws.numel(),
+                                        stream), "dmpc_rollout_adj")
+        solver._event_end(ev, "k_rollout_adj")
+    grads = spec.gradients()
+    return {k: grads[k] for k in keys}, gx0
+
+
+def _per_step_sweep(ctx, g_cost):
+    """The same sweep with one batched dmpc_solve_adj launch per step (host loop)."""
+    roll, call, st, keys = ctx.roll, ctx.call, ctx.st, ctx.keys
+    solver = roll.solver
+    B, K, nx, nu, T = call.B, call.K, call.nx, call.nu, roll.num_sim_steps
+    go = g_cost.to(torch.float64).reshape(B, 1)
+    akeys = list(keys) + (["initial_state"] if roll.through_state and "initial_state" not in keys else [])
+    acc = {}
+    lam = 2.0 * go * st.x[T]
+    for k in reversed(range(T)):
+        u = st.controls[k, :, 0]
+        g_u = 2.0 * go * u + torch.einsum("bij,bi->bj", st.Bm, lam)
+        dlu = torch.zeros(B, K, nu, dtype=torch.float64, device=u.device)
+        dlu[:, 0] = g_u
+        g = _lib.Group.from_buffer_copy(call.group)
+        g.initial_state = _ptr(st.x[k])
+        g.states, g.controls, g.dual = _ptr(st.states[k]), _ptr(st.controls[k]), _ptr(st.dual[k])
+        g.lin_states, g.lin_controls = _ptr(st.lin_states[k]), _ptr(st.lin_controls[k])
+        g.status, g.num_iter, g.convergence_error = _ptr(st.status[k]), _ptr(st.num_iter[k]), _ptr(st.conv[k])
+        g.convergence_errors, g.linesearch_alphas = _ptr(st.conv_hist[k]), _ptr(st.alpha_hist[k])
+        g.num_pcg_iters = _ptr(st.pcg_hist[k])
+        view = SimpleNamespace(group=g, states=st.states[k], B=B, K=K, nx=nx, nu=nu)
+        dbg = torch.zeros(B, K, nx, dtype=torch.float64, device=u.device)
+        grads = solver._run_adj(view, None, dlu, dbg, akeys) if akeys else {}
+        for key in keys:
+            acc[key] = grads[key] if key not in acc else acc[key] + grads[key]
+        lam = torch.einsum("bij,bi->bj", st.A, lam)
+        if roll.through_state:
+            lam = lam + grads["initial_state"]
+        if k >= 1:
+            lam = lam + 2.0 * go * st.x[k]
+    return acc, lam
 
 
 class ClosedLoopRollout:
@@ -137,12 +177,14 @@ class ClosedLoopRollout:
     ``sum_k |x_{k+1}|^2 + |u_k|^2`` per instance (shape ``(B,)``), differentiable with
     respect to ``weights`` (any key ``SQPSolver.solve`` accepts) and ``initial_states``.
     ``warm_start`` starts each solve from the previous step's solution, as the
-    reference's ``warm_start`` flag does.  After a call, ``last`` holds every step's
+    reference's ``warm_start`` flag does.  The backward pass is one launch per parameter
+    chunk (``dmpc_rollout_adj``); ``fused_backward=False`` runs the same sweep as one
+    ``dmpc_solve_adj`` launch per step instead.  After a call, ``last`` holds every step's
     solution (``states``, ``controls``, ``x`` ...) and iteration counts.
     """
 
     def __init__(self, solver: SQPSolver, sim_A, sim_B, sim_b, num_sim_steps: int, warm_start: bool = True,
-                 through_state: bool = False):
+                 through_state: bool = False, fused_backward: bool = True):
         if num_sim_steps < 1:
             raise ValueError("num_sim_steps must be >= 1")
         self.solver = solver
@@ -150,11 +192,14 @@ class ClosedLoopRollout:
         self.num_sim_steps = int(num_sim_steps)
         self.warm_start = bool(warm_start)
         self.through_state = bool(through_state)
+        self.fused_backward = bool(fused_backward)
         self.last = None
 
     def __call__(self, initial_states: torch.Tensor, problem_params: Dict, weights: Optional[Dict] = None,
                  initial_guess: Optional[SQPSolution] = None) -> torch.Tensor:
         weights = weights or {}
+        if "initial_state" in weights:
+            raise ValueError("the rollout's initial states are `initial_states`, not a weight")
         x0 = torch.as_tensor(initial_states, dtype=torch.float64)
         keys = sorted(weights.keys())
         vals = [torch.as_tensor(weights[k], dtype=torch.float64, device=x0.device) for k in keys]

@@ -188,6 +188,15 @@ typedef struct {
   double* running_cost;             /* (batch) */
 } dmpc_rollout;
 
+/* Reverse sweep of a rollout's gradient.  All pointers are device memory. */
+typedef struct {
+  const double* cost_cotangent;     /* (batch) dL/d running_cost */
+  int32_t through_state;            /* 1: add each solve's dL/dx_k (the reference's custom VJP does not) */
+  double* scratch_dl_dcontrols;     /* (batch, K, nu) working array */
+  double* scratch_dual;             /* (batch, K, nx) working array */
+  double* g_initial_state;          /* (batch, nx) dL/dx_0, optional */
+} dmpc_rollout_adjoint;
+
 int dmpc_abi_version(void);
 const char* dmpc_error_string(int code);
 /* Name of the last CUDA runtime error an entry point returned DMPC_ERR_CUDA for on the
@@ -277,6 +286,18 @@ int dmpc_compute_gamma(int batch, int N, int nx, int nu, const double* As_x_Qinv
  * the rollout's step arrays, so that the adjoint of step k is dmpc_solve_adj on a group
  * view pointing at them.  Same workspace as dmpc_solve_fwd for `group`. */
 int dmpc_rollout_fwd(const dmpc_group* group, const dmpc_rollout* rollout, const dmpc_solver_params* params,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Gradient of the rollout of dmpc_rollout_fwd (jax.grad of the reference's scan), every step
+ * of every instance in ONE launch: a reverse sweep over the steps that runs the adjoint of
+ * each step's solve (dmpc_solve_adj, at the solution and linearization point the forward kept
+ * in `rollout`) for the control cotangent that the simulator chain gives it.  `adj` selects
+ * the parameter gradients as for dmpc_solve_adj; they are ACCUMULATED over the steps into
+ * adj's g_* outputs, which the caller zeroes first.  adj's dl_dstates, dl_dcontrols,
+ * dual_backward_guess, dual_backward, g_initial_state, adj_states, adj_controls and
+ * num_pcg_iter are not used.  Same workspace as dmpc_solve_adj for `group`. */
+int dmpc_rollout_adj(const dmpc_group* group, const dmpc_rollout* rollout, const dmpc_adjoint* adj,
+                     const dmpc_rollout_adjoint* rollout_adjoint, const dmpc_solver_params* params,
                      void* workspace, size_t workspace_bytes, void* stream);
 
 /* get_states_controls_from_kkt_multipliers (pcg.py:290-348), general dense matrices:

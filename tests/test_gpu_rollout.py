@@ -1,7 +1,8 @@
-"""Fused closed-loop rollout (dmpc_rollout_fwd + a reverse sweep of dmpc_solve_adj).
+"""Fused closed-loop rollout (dmpc_rollout_fwd forward, dmpc_rollout_adj reverse sweep).
 
 * Every step of the one-launch rollout equals the same step run as a separate
-  SQPSolver.solve call from the host (same kernels, same guess chain).
+  SQPSolver.solve call from the host (same kernels, same guess chain), and the
+  one-launch backward sweep equals the sweep run as one adjoint launch per step.
 * Running cost, per-step controls and gradients w.r.t. cost weights and the simulator's
   model matrix match the oracle's rollout (oracle/rollout.py), whose gradient is pinned
   to finite differences on the CPU: FP64 to 1e-9 / 1e-7, mixed precision at PCG tolerance
@@ -82,6 +83,22 @@ def test_rollout_cost_and_gradients_match_oracle(precision, warm, through_state)
         assert rel_err(roll.last.controls[k][:, 0], ous[k]) < ctol, k
     for k in wkeys:
         assert rel_err(w[k].grad, ow[k].grad) < gtol, k
+
+
+@pytest.mark.parametrize("through_state", [False, True])
+def test_fused_backward_equals_per_step_adjoint_sweep(through_state):
+    """dmpc_rollout_adj (one launch) against the same sweep as one dmpc_solve_adj per step."""
+    dyn, st, bt, sp, (A, Bm, b), solver, p = _setup("fp64", True, B=4)
+    grads = []
+    for fused in (True, False):
+        w = {KW: p[KW].clone().requires_grad_(True), "A": p["A"].clone().requires_grad_(True)}
+        x0 = p["initial_state"].clone().requires_grad_(True)
+        roll = ClosedLoopRollout(solver, A.to(DEV), Bm.to(DEV), b.to(DEV), 4, through_state=through_state,
+                                 fused_backward=fused)
+        (roll(x0, p, w) * torch.arange(1, 5, device=DEV)).sum().backward()
+        grads.append((w[KW].grad, w["A"].grad, x0.grad))
+    for a, c in zip(*grads):
+        assert rel_err(a, c) < 1e-12
 
 
 def test_reference_benchmark_configuration_matches_oracle():
