@@ -47,7 +47,7 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU-baseline sample")
     ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
-    ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress", "rollout"],
+    ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress", "rollout", "rollout_spacecraft"],
                     help="quadrotor = the headline; the others report the remaining workload shapes")
     return ap.parse_args()
 
@@ -566,6 +566,37 @@ def run_other_workload(args):
                         "source": "benchmarking/reinforcement-learning/timing_results/"
                                   "timing_64_40_12_pcg=1e-12_warmstart=True/diffmpc_cuda:0_{fwd,bwd}.npy (median of 100)"},
                     max_rel_cost_diff_fused_vs_host_loop=float((c_fb - c_h).abs().max() / c_h.abs().max()),
+                    pcg_iters_per_solve=float(roll.last.pcg_hist.double().sum() / (B * T)))
+    elif args.workload == "rollout_spacecraft":
+        from diffmpc_b200.rollout import ClosedLoopRollout
+
+        B = args.batch if args.batch != 4096 else 16
+        T = 20
+        dyn, st, bt, sp = workloads.rl_spacecraft(B=B)
+        solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp, device=dev)
+        p = workloads.to_device(bt, dev)
+        keys = ["weights_penalization_reference_state_trajectory", "weights_penalization_control_squared"]
+        roll = ClosedLoopRollout(solver, num_sim_steps=T, simulator="model", state_weight=10.0)
+
+        def run(grad):
+            w = {k: p[k].clone().requires_grad_(grad) for k in keys}
+            c = roll(p["initial_state"], p, w)
+            if grad:
+                c.sum().backward()
+            return c
+
+        ms_f, _ = _timed(lambda: run(False), args.steps, args.warmup)
+        ms_fb, _ = _timed(lambda: run(True), args.steps, args.warmup)
+        line.update(metric="closed-loop MPC rollout, spacecraft nx=3 N=39, 20 steps, model Euler simulator, "
+                           "B=%d: MPC solves/s (B*steps per second), fwd+bwd through the rollout" % B,
+                    value=B * T / (ms_fb * 1e-3), ms_per_step=ms_fb, batch=B, sim_steps=T,
+                    fwd_only_solves_per_s=B * T / (ms_f * 1e-3), fwd_only_ms=ms_f,
+                    reference_recorded={
+                        "fwd_ms_per_rollout": 5.5, "fwd_bwd_ms_per_rollout": 8.8,
+                        "config": "batch and horizon unrecorded (script defaults B=16, 40 knots, 20 steps), "
+                                  "FP64 JAX on CPU (TFRT_CPU_0)",
+                        "source": "benchmarking/reinforcement-learning/spacecraft/timing_results/spacecraft_timing/"
+                                  "diffmpc_TFRT_CPU_0_{fwd,bwd}.npy (median)"},
                     pcg_iters_per_solve=float(roll.last.pcg_hist.double().sum() / (B * T)))
     else:  # stress
         B = args.batch if args.batch != 4096 else 1024

@@ -22,6 +22,7 @@ DMPC_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 MODEL_IDS = {"linear": 0, "quadrotor": 1, "spacecraft": 2, "attitude": 3, "cartpole": 4}
 PREC_FP64, PREC_MIXED = 0, 1
+SIM_LINEAR, SIM_MODEL = 0, 1
 
 EXPORTED_SYMBOLS = (
     "dmpc_abi_version",
@@ -127,6 +128,10 @@ class Rollout(ctypes.Structure):
     _fields_ = [
         ("num_steps", _i32),
         ("warm_start", _i32),
+        ("simulator", _i32),
+        ("reserved", _i32),
+        ("cost_state_weight", _f64),
+        ("cost_control_weight", _f64),
         ("sim_A", _p),
         ("sim_B", _p),
         ("sim_b", _p),

@@ -1308,6 +1308,40 @@ __global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevA
 }
 
 // ---------------------------------------------------------------- closed-loop rollout
+// One Euler step of the instance's model as the rollout's simulator: sum_i lam_i d(x+_i)/dz_d
+// for the direction z_d of (x, u) (d < nx: state, else control), by one Dual evaluation.
+// `s` must carry scheme DMPC_EULER.
+template <int MODEL>
+__device__ __noinline__ double sim_vjp_item(const Inst& s, const double* x, const double* u, const double* lam, int d) {
+  constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
+  const int nx = MODEL == DMPC_MODEL_LINEAR ? s.nx : MX, nu = MODEL == DMPC_MODEL_LINEAR ? s.nu : MU;
+  Dual xd[MX], ud[MU], xn[MX];
+  for (int j = 0; j < nx; ++j) xd[j] = Dual(x[j], j == d ? 1.0 : 0.0);
+  for (int j = 0; j < nu; ++j) ud[j] = Dual(u[j], nx + j == d ? 1.0 : 0.0);
+  if (MODEL == DMPC_MODEL_LINEAR) {
+    predict_next_state_linear(s, xd, ud, xn);
+  } else {
+    Dual p[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) p[k] = Dual(k < s.P ? s.mp[k] : 0.0);
+    predict_next_state<Dual, MODEL>(DMPC_EULER, s.dt, nx, nu, xd, ud, p, xn);
+  }
+  double acc = 0.0;
+  for (int i = 0; i < nx; ++i) acc += lam[i] * xn[i].d;
+  return acc;
+}
+
+__device__ double sim_vjp(const Inst& s, const double* x, const double* u, const double* lam, int d) {
+  switch (s.model) {
+    case DMPC_MODEL_LINEAR: return sim_vjp_item<DMPC_MODEL_LINEAR>(s, x, u, lam, d);
+    case DMPC_MODEL_QUADROTOR: return sim_vjp_item<DMPC_MODEL_QUADROTOR>(s, x, u, lam, d);
+    case DMPC_MODEL_SPACECRAFT: return sim_vjp_item<DMPC_MODEL_SPACECRAFT>(s, x, u, lam, d);
+    case DMPC_MODEL_ATTITUDE: return sim_vjp_item<DMPC_MODEL_ATTITUDE>(s, x, u, lam, d);
+    case DMPC_MODEL_CARTPOLE: return sim_vjp_item<DMPC_MODEL_CARTPOLE>(s, x, u, lam, d);
+  }
+  return 0.0;
+}
+
 // The group as seen by simulation step k: initial state x_k, and solution, linearization
 // point, status and histories in step k's slices of the rollout arrays.
 __device__ inline dmpc_group rollout_step_view(const dmpc_group& g0, const dmpc_rollout& ra, int k, int Kmax, int mi) {
@@ -1331,8 +1365,9 @@ __device__ inline dmpc_group rollout_step_view(const dmpc_group& g0, const dmpc_
 
 // benchmark_diffmpc.py:140-175 (lax.scan of rollout_step, vmapped over instances), one CTA
 // per instance for all simulation steps: solve the MPC from x_k (warm-started from step
-// k-1's solution, or from the initial guess), apply u_k = controls[0], simulate
-// x_{k+1} = A x_k + B u_k + b and add |x_{k+1}|^2 + |u_k|^2 to the running cost.  Every
+// k-1's solution, or from the initial guess), apply u_k = controls[0], simulate x_{k+1}
+// (x_{k+1} = A x_k + B u_k + b, or an Euler step of the model as in
+// spacecraft/benchmark_diffmpc.py:87-89) and add ws |x_{k+1}|^2 + wc |u_k|^2.  Every
 // step's solution and last linearization point are kept for the adjoint sweep.
 __global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ DevArgs args,
                                                         const __grid_constant__ dmpc_rollout ra, void* ws) {
@@ -1376,24 +1411,32 @@ __global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ 
     __syncthreads();
     sqp_forward(G, sh_g, ii, args.p, ws, smem);
     __syncthreads();
-    // simulator step and running cost (reward = -(|x_{k+1}|^2 + |u_k|^2))
+    // simulator step and running cost (the negated reward)
     const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
     const double* u = sh_g.controls + ou;  // controls[0]
     double* xn = ra.step_initial_state + ((size_t)(k + 1) * B + ii) * nx;
-    const double* A = ra.sim_A + (size_t)ii * nx * nx;
-    const double* Bm = ra.sim_B + (size_t)ii * nx * nu;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-      double a = ra.sim_b[(size_t)ii * nx + i];
-      for (int j = 0; j < nx; ++j) a += A[i * nx + j] * x[j];
-      for (int j = 0; j < nu; ++j) a += Bm[i * nu + j] * u[j];
-      xn[i] = a;
+    if (ra.simulator == DMPC_SIM_MODEL) {
+      if (threadIdx.x == 0) {
+        Inst se = make_inst(G, sh_g, ii, ws, nullptr);
+        se.scheme = DMPC_EULER;
+        next_state_value(se, x, u, xn);
+      }
+    } else {
+      const double* A = ra.sim_A + (size_t)ii * nx * nx;
+      const double* Bm = ra.sim_B + (size_t)ii * nx * nu;
+      for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        double a = ra.sim_b[(size_t)ii * nx + i];
+        for (int j = 0; j < nx; ++j) a += A[i * nx + j] * x[j];
+        for (int j = 0; j < nu; ++j) a += Bm[i * nu + j] * u[j];
+        xn[i] = a;
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      double c = 0.0;
-      for (int i = 0; i < nx; ++i) c += xn[i] * xn[i];
-      for (int j = 0; j < nu; ++j) c += u[j] * u[j];
-      sh_cost += c;
+      double cx = 0.0, cu = 0.0;
+      for (int i = 0; i < nx; ++i) cx += xn[i] * xn[i];
+      for (int j = 0; j < nu; ++j) cu += u[j] * u[j];
+      sh_cost += ra.cost_state_weight * cx + ra.cost_control_weight * cu;
     }
     __syncthreads();
   }
@@ -1533,10 +1576,11 @@ __global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevA
 }
 
 // Reverse sweep of the rollout's gradient (what jax.grad of the reference's scan computes):
-// with lam_T = 2 c x_T (c = dL/d running cost), for k = T-1 .. 0
-//   dl/du_0 of step k  = 2 c u_k + B^T lam_{k+1}
+// with lam_T = 2 c ws x_T (c = dL/d running cost), F the simulator step, for k = T-1 .. 0
+//   dl/du_0 of step k  = 2 c wc u_k + (dF/du)^T lam_{k+1}
 //   adjoint of step k's solve, parameter gradients accumulated into adj's outputs
-//   lam_k = A^T lam_{k+1} + 2 c x_k (k >= 1) [+ the solve's dL/dx_0 if through_state]
+//   lam_k = (dF/dx)^T lam_{k+1} + 2 c ws x_k (k >= 1) [+ the solve's dL/dx_0 if through_state]
+// (dF/dz)^T lam is formed by one Dual evaluation per direction for the model simulator.
 // and dL/dx_0 = lam_0.  One CTA per instance, all steps in one launch.
 __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ DevArgs args,
                                                         const __grid_constant__ dmpc_rollout ra,
@@ -1551,10 +1595,11 @@ __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ 
   const size_t ox = (size_t)ii * Kmax * nx, ou = (size_t)ii * Kmax * nu;
   __shared__ dmpc_group sh_g;
   __shared__ dmpc_adjoint sh_a;
-  __shared__ double sh_lam[DMPC_MAX_NX], sh_nxt[DMPC_MAX_NX];
+  __shared__ double sh_lam[DMPC_MAX_NX], sh_vjp[DMPC_MAX_NX + DMPC_MAX_NU];
   const double c = rr.cost_cotangent[ii];
+  const double cs = 2.0 * c * ra.cost_state_weight, cc = 2.0 * c * ra.cost_control_weight;
   const int T = ra.num_steps;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = 2.0 * c * ra.step_initial_state[((size_t)T * B + ii) * nx + i];
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = cs * ra.step_initial_state[((size_t)T * B + ii) * nx + i];
   for (int w = threadIdx.x; w < Kmax * nu; w += blockDim.x) rr.scratch_dl_dcontrols[ou + w] = 0.0;
   __syncthreads();
   for (int k = T - 1; k >= 0; --k) {
@@ -1573,26 +1618,37 @@ __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ 
     }
     __syncthreads();
     const double* u = sh_g.controls + ou;  // u_k = controls[0]
-    const double* Bm = ra.sim_B + (size_t)ii * nx * nu;
-    for (int j = threadIdx.x; j < nu; j += blockDim.x) {
-      double v = 2.0 * c * u[j];
-      for (int i = 0; i < nx; ++i) v += Bm[i * nu + j] * sh_lam[i];
-      rr.scratch_dl_dcontrols[ou + j] = v;
+    const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
+    // sh_vjp = [dx_{k+1}/dx_k, dx_{k+1}/du_k]^T lam_{k+1}
+    if (ra.simulator == DMPC_SIM_MODEL) {
+      for (int d = threadIdx.x; d < nx + nu; d += blockDim.x) {
+        Inst se = make_inst(G, sh_g, ii, ws, nullptr);
+        se.scheme = DMPC_EULER;
+        sh_vjp[d] = sim_vjp(se, x, u, sh_lam, d);
+      }
+    } else {
+      const double* A = ra.sim_A + (size_t)ii * nx * nx;
+      const double* Bm = ra.sim_B + (size_t)ii * nx * nu;
+      for (int d = threadIdx.x; d < nx + nu; d += blockDim.x) {
+        double v = 0.0;
+        if (d < nx)
+          for (int j = 0; j < nx; ++j) v += A[j * nx + d] * sh_lam[j];
+        else
+          for (int i = 0; i < nx; ++i) v += Bm[i * nu + (d - nx)] * sh_lam[i];
+        sh_vjp[d] = v;
+      }
     }
+    __syncthreads();
+    for (int j = threadIdx.x; j < nu; j += blockDim.x) rr.scratch_dl_dcontrols[ou + j] = cc * u[j] + sh_vjp[nx + j];
     __syncthreads();
     sqp_adjoint(G, sh_g, sh_a, ii, args.p, ws, smem, true);
     __syncthreads();
-    const double* A = ra.sim_A + (size_t)ii * nx * nx;
-    const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-      double v = 0.0;
-      for (int j = 0; j < nx; ++j) v += A[j * nx + i] * sh_lam[j];
+      double v = sh_vjp[i];
       if (rr.through_state) v += rr.scratch_dual[ox + i];  // the solve's dL/dx_0 = lam~_0
-      if (k >= 1) v += 2.0 * c * x[i];
-      sh_nxt[i] = v;
+      if (k >= 1) v += cs * x[i];
+      sh_lam[i] = v;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = sh_nxt[i];
     __syncthreads();
   }
   if (rr.g_initial_state)
@@ -1968,7 +2024,7 @@ int cuda_rc(cudaError_t e) {
 constexpr size_t kStaticSmemReserve = 2048;
 // (the rollout kernels also keep the per-step group and adjoint views and the state
 // cotangent there)
-static_assert(sizeof(Inst) + sizeof(dmpc_group) + sizeof(dmpc_adjoint) + 2 * DMPC_MAX_NX * sizeof(double) +
+static_assert(sizeof(Inst) + sizeof(dmpc_group) + sizeof(dmpc_adjoint) + (2 * DMPC_MAX_NX + DMPC_MAX_NU) * sizeof(double) +
                       2 * sizeof(double) + 64 <= kStaticSmemReserve,
               "static shared memory reserve too small");
 
@@ -2176,7 +2232,9 @@ int dmpc_rollout_adj(const dmpc_group* group, const dmpc_rollout* ro, const dmpc
                      const dmpc_rollout_adjoint* rr, const dmpc_solver_params* params, void* workspace,
                      size_t workspace_bytes, void* stream) {
   if (!group || !ro || !adj || !rr || ro->num_steps < 1) return DMPC_ERR_INVALID;
-  if (!ro->sim_A || !ro->sim_B || !ro->step_initial_state || !ro->step_states || !ro->step_controls ||
+  if (ro->simulator != DMPC_SIM_LINEAR && ro->simulator != DMPC_SIM_MODEL) return DMPC_ERR_INVALID;
+  if (ro->simulator == DMPC_SIM_LINEAR && (!ro->sim_A || !ro->sim_B)) return DMPC_ERR_INVALID;
+  if (!ro->step_initial_state || !ro->step_states || !ro->step_controls ||
       !ro->step_dual || !ro->step_lin_states || !ro->step_lin_controls || !ro->step_status || !ro->step_num_iter ||
       !ro->step_convergence_error || !ro->step_convergence_errors || !ro->step_linesearch_alphas ||
       !ro->step_num_pcg_iters || !rr->cost_cotangent || !rr->scratch_dl_dcontrols || !rr->scratch_dual)
@@ -2202,7 +2260,9 @@ int dmpc_rollout_adj(const dmpc_group* group, const dmpc_rollout* ro, const dmpc
 int dmpc_rollout_fwd(const dmpc_group* group, const dmpc_rollout* ro, const dmpc_solver_params* params,
                      void* workspace, size_t workspace_bytes, void* stream) {
   if (!group || !ro || ro->num_steps < 1) return DMPC_ERR_INVALID;
-  if (!ro->sim_A || !ro->sim_B || !ro->sim_b || !ro->step_initial_state || !ro->step_states || !ro->step_controls ||
+  if (ro->simulator != DMPC_SIM_LINEAR && ro->simulator != DMPC_SIM_MODEL) return DMPC_ERR_INVALID;
+  if (ro->simulator == DMPC_SIM_LINEAR && (!ro->sim_A || !ro->sim_B || !ro->sim_b)) return DMPC_ERR_INVALID;
+  if (!ro->step_initial_state || !ro->step_states || !ro->step_controls ||
       !ro->step_dual || !ro->step_lin_states || !ro->step_lin_controls || !ro->step_status || !ro->step_num_iter ||
       !ro->step_convergence_error || !ro->step_convergence_errors || !ro->step_linesearch_alphas ||
       !ro->step_num_pcg_iters || !ro->running_cost)

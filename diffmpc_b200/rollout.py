@@ -58,16 +58,19 @@ class _RolloutFunction(torch.autograd.Function):
         mi = solver.maxiter
         f64 = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)  # noqa: E731
         i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
+        linear = roll.simulator == "linear"
         st = SimpleNamespace(
-            A=_per_instance(roll.sim_A, B, (nx, nx), dev),
-            Bm=_per_instance(roll.sim_B, B, (nx, nu), dev),
-            b=_per_instance(roll.sim_b, B, (nx,), dev),
+            A=_per_instance(roll.sim_A, B, (nx, nx), dev) if linear else None,
+            Bm=_per_instance(roll.sim_B, B, (nx, nu), dev) if linear else None,
+            b=_per_instance(roll.sim_b, B, (nx,), dev) if linear else None,
             x=f64(T + 1, B, nx), states=f64(T, B, K, nx), controls=f64(T, B, K, nu), dual=f64(T, B, K, nx),
             lin_states=f64(T, B, K, nx), lin_controls=f64(T, B, K, nu), status=i32(T, B), num_iter=i32(T, B),
             conv=f64(T, B), conv_hist=f64(T, B, mi), alpha_hist=f64(T, B, mi), pcg_hist=i32(T, B, mi), cost=f64(B),
         )
         r = _lib.Rollout()
         r.num_steps, r.warm_start = T, 1 if roll.warm_start else 0
+        r.simulator = _lib.SIM_LINEAR if linear else _lib.SIM_MODEL
+        r.cost_state_weight, r.cost_control_weight = roll.state_weight, roll.control_weight
         r.sim_A, r.sim_B, r.sim_b = _ptr(st.A), _ptr(st.Bm), _ptr(st.b)
         r.step_initial_state, r.step_states, r.step_controls = _ptr(st.x), _ptr(st.states), _ptr(st.controls)
         r.step_dual, r.step_lin_states, r.step_lin_controls = _ptr(st.dual), _ptr(st.lin_states), _ptr(st.lin_controls)
@@ -92,7 +95,7 @@ class _RolloutFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g_cost):
         roll, call, st, keys = ctx.roll, ctx.call, ctx.st, ctx.keys
-        if roll.fused_backward:
+        if roll.fused_backward or roll.simulator != "linear":
             acc, gx0 = _fused_sweep(ctx, g_cost)
         else:
             acc, gx0 = _per_step_sweep(ctx, g_cost)
@@ -141,12 +144,13 @@ def _per_step_sweep(ctx, g_cost):
     solver = roll.solver
     B, K, nx, nu, T = call.B, call.K, call.nx, call.nu, roll.num_sim_steps
     go = g_cost.to(torch.float64).reshape(B, 1)
+    ws_, wc_ = roll.state_weight, roll.control_weight
     akeys = list(keys) + (["initial_state"] if roll.through_state and "initial_state" not in keys else [])
     acc = {}
-    lam = 2.0 * go * st.x[T]
+    lam = 2.0 * ws_ * go * st.x[T]
     for k in reversed(range(T)):
         u = st.controls[k, :, 0]
-        g_u = 2.0 * go * u + torch.einsum("bij,bi->bj", st.Bm, lam)
+        g_u = 2.0 * wc_ * go * u + torch.einsum("bij,bi->bj", st.Bm, lam)
         dlu = torch.zeros(B, K, nu, dtype=torch.float64, device=u.device)
         dlu[:, 0] = g_u
         g = _lib.Group.from_buffer_copy(call.group)
@@ -165,28 +169,43 @@ def _per_step_sweep(ctx, g_cost):
         if roll.through_state:
             lam = lam + grads["initial_state"]
         if k >= 1:
-            lam = lam + 2.0 * go * st.x[k]
+            lam = lam + 2.0 * ws_ * go * st.x[k]
     return acc, lam
 
 
 class ClosedLoopRollout:
-    """MPC-in-the-loop rollout of ``num_sim_steps`` steps with the linear simulator
-    ``x+ = sim_A x + sim_B u + sim_b`` (each shared by the batch or given per instance).
+    """MPC-in-the-loop rollout of ``num_sim_steps`` steps.
+
+    ``simulator="linear"``: ``x+ = sim_A x + sim_B u + sim_b`` (each shared by the batch or
+    given per instance), as in benchmark_diffmpc.py:148-150.  ``simulator="model"``: one
+    Euler step ``x+ = x + dt f(x, u)`` of the solver's own model with each instance's ``dt``
+    and model parameters, as in spacecraft/benchmark_diffmpc.py:87-89.  The simulator uses
+    the model parameters the solves see (a weight that overrides one applies to both) and is
+    not differentiated with respect to them.
 
     ``rollout(initial_states, problem_params, weights)`` returns the running cost
-    ``sum_k |x_{k+1}|^2 + |u_k|^2`` per instance (shape ``(B,)``), differentiable with
-    respect to ``weights`` (any key ``SQPSolver.solve`` accepts) and ``initial_states``.
+    ``sum_k state_weight |x_{k+1}|^2 + control_weight |u_k|^2`` per instance (shape ``(B,)``;
+    the reference scripts' reward is its negative, with weights 1, 1 for the linear and
+    10, 1 for the spacecraft benchmark), differentiable with respect to ``weights`` (any key
+    ``SQPSolver.solve`` accepts) and ``initial_states``.
     ``warm_start`` starts each solve from the previous step's solution, as the
     reference's ``warm_start`` flag does.  The backward pass is one launch per parameter
-    chunk (``dmpc_rollout_adj``); ``fused_backward=False`` runs the same sweep as one
-    ``dmpc_solve_adj`` launch per step instead.  After a call, ``last`` holds every step's
+    chunk (``dmpc_rollout_adj``); for the linear simulator ``fused_backward=False`` runs
+    the same sweep as one ``dmpc_solve_adj`` launch per step instead.  After a call, ``last`` holds every step's
     solution (``states``, ``controls``, ``x`` ...) and iteration counts.
     """
 
-    def __init__(self, solver: SQPSolver, sim_A, sim_B, sim_b, num_sim_steps: int, warm_start: bool = True,
-                 through_state: bool = False, fused_backward: bool = True):
+    def __init__(self, solver: SQPSolver, sim_A=None, sim_B=None, sim_b=None, num_sim_steps: int = 1,
+                 warm_start: bool = True, through_state: bool = False, fused_backward: bool = True,
+                 simulator: str = "linear", state_weight: float = 1.0, control_weight: float = 1.0):
         if num_sim_steps < 1:
             raise ValueError("num_sim_steps must be >= 1")
+        if simulator not in ("linear", "model"):
+            raise ValueError("simulator must be 'linear' or 'model'")
+        if simulator == "linear" and (sim_A is None or sim_B is None or sim_b is None):
+            raise ValueError("the linear simulator needs sim_A, sim_B and sim_b")
+        self.simulator = simulator
+        self.state_weight, self.control_weight = float(state_weight), float(control_weight)
         self.solver = solver
         self.sim_A, self.sim_B, self.sim_b = sim_A, sim_B, sim_b
         self.num_sim_steps = int(num_sim_steps)

@@ -21,7 +21,7 @@ import math
 import numpy as np
 import torch
 
-from .dynamics import LinearDynamics, QuadrotorDynamics, SpacecraftAttitudeDynamics
+from .dynamics import LinearDynamics, QuadrotorDynamics, SpacecraftAttitudeDynamics, SpacecraftDynamics
 from .problem import load_solver_params
 
 F64 = torch.float64
@@ -145,6 +145,31 @@ def rl_linear(B=1024, seed=1005, nx=8, nu=4, N=39, warm_start=True):
     sp["linesearch"] = True
     sp["linesearch_alphas"] = [1.0]
     return dyn, _static_of(batched), batched, sp, (_t(A), _t(Bm), _t(b))
+
+
+def rl_spacecraft(B=16, seed=1006, N=39):
+    """Closed-loop benchmark problem of the reference's spacecraft script
+    (spacecraft/benchmark_diffmpc.py:30-60, spacecraft/utils.py): angular-rate spacecraft with
+    one inertia vector shared by the batch, inertia ~ U[1, 10]^3, x0 ~ U[-0.1, 0.1]^3, the
+    spacecraft.yaml weights (Q = I, R = I, dt = 0.1, Euler), zero references and terminal
+    weight, horizon N = 39 (40 knots); one SQP iteration with the line search at alpha = 1,
+    PCG tolerance 1e-12.  The rollout simulates with the model's own Euler step and the cost
+    10 |x|^2 + |u|^2.  Returns (dynamics, static params, batched params, solver params)."""
+    rng = np.random.default_rng(seed)
+    J = 1.0 + 9.0 * rng.random(3)
+    x0 = -0.1 + 0.2 * rng.random((B, 3))
+    K = N + 1
+    batched = _base(
+        N, np.full(B, 0.1), 0, x0, np.zeros((B, 3)), np.zeros((B, K, 3)), np.zeros((B, K, 3)),
+        np.ones((B, 3)), np.ones((B, 3)), np.zeros((B, 3)), False,
+        {"inertia_vector": np.repeat(J[None], B, axis=0)},
+    )
+    sp = load_solver_params("sqp.yaml")
+    sp["num_scp_iteration_max"] = 1
+    sp["pcg"]["tol_epsilon"] = 1e-12
+    sp["linesearch"] = True
+    sp["linesearch_alphas"] = [1.0]
+    return SpacecraftDynamics(), _static_of(batched), batched, sp
 
 
 def attitude(B=1024, seed=1001, N=50):

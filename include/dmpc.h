@@ -164,15 +164,23 @@ typedef struct dmpc_adjoint {
 /* Closed-loop rollout (benchmarking/reinforcement-learning/benchmark_diffmpc.py:140-175, the
  * rollout_step scanned with lax.scan and vmapped over instances).  For k = 0..num_steps-1:
  * solve the MPC with initial state x_k starting from step k-1's solution (warm_start) or from
- * the group's initial guess, apply u_k = controls[0], simulate x_{k+1} = A x_k + B u_k + b and
- * add |x_{k+1}|^2 + |u_k|^2 to the running cost.  All pointers are device memory; K = horizon+1,
+ * the group's initial guess, apply u_k = controls[0], simulate x_{k+1} (see `simulator`) and add
+ * cost_state_weight |x_{k+1}|^2 + cost_control_weight |u_k|^2 to the running cost (the reference
+ * scripts' negated reward: weights 1, 1 for the linear benchmark, 10, 1 for the spacecraft one).  All pointers are device memory; K = horizon+1,
  * T = num_steps. */
+#define DMPC_SIM_LINEAR 0 /* x+ = A x + B u + b (benchmark_diffmpc.py:148-150) */
+#define DMPC_SIM_MODEL 1  /* x+ = x + dt f(x, u): one Euler step of the group's model with each instance's
+                             dt and model parameters (spacecraft/benchmark_diffmpc.py:87-89) */
 typedef struct {
   int32_t num_steps;                /* T >= 1 */
   int32_t warm_start;               /* 1: step k starts from step k-1's solution */
-  const double* sim_A;              /* (batch, nx, nx) discrete simulator */
-  const double* sim_B;              /* (batch, nx, nu) */
-  const double* sim_b;              /* (batch, nx) */
+  int32_t simulator;                /* DMPC_SIM_LINEAR or DMPC_SIM_MODEL */
+  int32_t reserved;                 /* 0 */
+  double cost_state_weight;         /* running cost += cost_state_weight |x_{k+1}|^2 */
+  double cost_control_weight;       /*               + cost_control_weight |u_k|^2 */
+  const double* sim_A;              /* (batch, nx, nx) DMPC_SIM_LINEAR only */
+  const double* sim_B;              /* (batch, nx, nu) DMPC_SIM_LINEAR only */
+  const double* sim_b;              /* (batch, nx)     DMPC_SIM_LINEAR only */
   double* step_initial_state;       /* (T+1, batch, nx): x_0 (copied from the group) .. x_T */
   double* step_states;              /* (T, batch, K, nx) solutions */
   double* step_controls;            /* (T, batch, K, nu) */

@@ -13,6 +13,7 @@ instead, which differentiates through the solve's dependence on it.
 """
 
 import torch
+from torch.func import vmap
 
 
 def _stop(sol):
@@ -22,9 +23,22 @@ def _stop(sol):
     )
 
 
+def _model_step(solver, problem_params, x, u):
+    """``x + dt f(x, u)`` with the solver's model and each instance's parameters
+    (spacecraft/benchmark_diffmpc.py:87-89)."""
+    model = solver.program.model
+    p = {k: problem_params[k] for k in model.param_keys}
+    f = vmap(model.state_dot)(x, u, p)
+    dt = torch.as_tensor(problem_params["discretization_resolution"], dtype=torch.float64).reshape(-1, 1)
+    return x + dt * f
+
+
 def rollout(solver, problem_params, initial_states, weights, A, Bm, b, num_steps, warm_start=True,
-            through_state=False):
-    """Returns (running cost (B,), [u_k], [x_k]); differentiable w.r.t. ``weights``."""
+            through_state=False, simulator="linear", state_weight=1.0, control_weight=1.0):
+    """Returns (running cost (B,), [u_k], [x_k]); differentiable w.r.t. ``weights``.
+    ``simulator="model"`` replaces ``A x + B u + b`` by an Euler step of the solver's model
+    (A, Bm, b unused); the cost is state_weight |x_{k+1}|^2 + control_weight |u_k|^2 (the
+    spacecraft script's reward is -(10 |x|^2 + |u|^2), spacecraft/utils.py)."""
     x = initial_states
     guess0 = solver.initial_guess({**problem_params, "initial_state": x.detach()})
     guess = guess0
@@ -36,8 +50,12 @@ def rollout(solver, problem_params, initial_states, weights, A, Bm, b, num_steps
         else:
             sol = solver.solve(guess, {**problem_params, "initial_state": x.detach()}, weights)
         u = sol.controls[:, 0]
-        x_new = torch.einsum("bij,bj->bi", A, x) + torch.einsum("bij,bj->bi", Bm, u) + b
-        cost = cost + (x_new ** 2).sum(-1) + (u ** 2).sum(-1)
+        if simulator == "model":
+            # the model parameters as the solve sees them, not differentiated through the simulator
+            x_new = _model_step(solver, {**problem_params, **{k: v.detach() for k, v in weights.items()}}, x, u)
+        else:
+            x_new = torch.einsum("bij,bj->bi", A, x) + torch.einsum("bij,bj->bi", Bm, u) + b
+        cost = cost + state_weight * (x_new ** 2).sum(-1) + control_weight * (u ** 2).sum(-1)
         guess = _stop(sol) if warm_start else guess0
         x = x_new
         us.append(u)

@@ -120,3 +120,38 @@ def test_reference_benchmark_configuration_matches_oracle():
     # mixed precision (the solver default) at the benchmark's PCG tolerance 1e-12
     assert rel_err(cost, ocost) < 1e-6
     assert rel_err(w[KW].grad, ow[KW].grad) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("through_state", [False, True])
+def test_model_simulator_rollout_matches_oracle(precision, through_state):
+    """Spacecraft with its own Euler step as the simulator and cost 10 |x|^2 + |u|^2
+    (spacecraft/benchmark_diffmpc.py:68-96)."""
+    dyn, st, bt, sp = workloads.rl_spacecraft(B=3, seed=13, N=20)
+    sp["precision"] = precision
+    # the spacecraft's states and controls are ~1e-2 and its weight gradients ~1e-4, so the
+    # absolute PCG tolerance must be tighter for the same relative accuracy: against eps = 1e-24
+    # the oracle's own controls move by 1.6e-6 at eps = 1e-13, and its w_x gradient by 9e-4 at
+    # 1e-13, 1.8e-5 at 1e-16 and 3e-7 at 1e-20
+    sp["pcg"]["tol_epsilon"] = 1e-20
+    solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp)
+    p = workloads.to_device(bt, DEV)
+    T = 4
+    wkeys = [KW, KU]
+    w = {k: p[k].clone().requires_grad_(True) for k in wkeys}
+    roll = ClosedLoopRollout(solver, num_sim_steps=T, simulator="model", state_weight=10.0,
+                             through_state=through_state)
+    cost = roll(p["initial_state"], p, w)
+    cost.sum().backward()
+    osolver = oracle_solver(dyn, st, sp)
+    op = tensor_params(bt)
+    ow = {k: op[k].clone().requires_grad_(True) for k in wkeys}
+    ocost, ous, _ = oracle_rollout(osolver, op, op["initial_state"], ow, None, None, None, T, warm_start=True,
+                                   through_state=through_state, simulator="model", state_weight=10.0)
+    ocost.sum().backward()
+    ctol, gtol = (1e-9, 1e-7) if precision == "fp64" else (1e-6, 1e-5)
+    assert rel_err(cost, ocost) < ctol
+    for k in range(T):
+        assert rel_err(roll.last.controls[k][:, 0], ous[k]) < ctol, k
+    for k in wkeys:
+        assert rel_err(w[k].grad, ow[k].grad) < gtol, k
