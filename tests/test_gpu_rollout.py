@@ -155,3 +155,41 @@ def test_model_simulator_rollout_matches_oracle(precision, through_state):
         assert rel_err(roll.last.controls[k][:, 0], ous[k]) < ctol, k
     for k in wkeys:
         assert rel_err(w[k].grad, ow[k].grad) < gtol, k
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rl_spacecraft_notebook_rollout_on_gpu(precision):
+    """notebooks/RL_spacecraft.ipynb cells 5-14 as one fused rollout: 2 spacecraft, 40 knots, 20
+    steps of the model's Euler step, reward -(10 |x|^2 + |u|^2), the shared weights updated once
+    with learning rate 1.  The recorded loss is -2.8196995973193135; the printed weights agree to
+    the adjoint's stopping tolerance (the oracle pin gives the same bound)."""
+    import numpy as np
+
+    from diffmpc_b200 import SpacecraftDynamics
+    from tests.test_oracle_pins import STATIC, _batched, _spacecraft_params
+
+    np.random.seed(0)
+    inertia = 1.0 + np.random.rand(3) * 9.0
+    x0s = -0.1 + np.random.rand(2, 3) * 0.2
+    p = _spacecraft_params(39)
+    p["inertia_vector"] = inertia
+    st = {k: (torch.as_tensor(np.asarray(v), dtype=torch.float64) if k not in STATIC else v) for k, v in p.items()}
+    from diffmpc_b200 import load_solver_params
+
+    sp = load_solver_params("sqp.yaml")
+    sp.update(num_scp_iteration_max=1, linesearch=True, linesearch_alphas=[1.0], precision=precision)
+    sp["pcg"]["tol_epsilon"] = 1e-12
+    solver = SQPSolver(OptimalControlProblem(SpacecraftDynamics(), st), params=sp)
+    bp = {k: v.to(DEV) for k, v in _batched(p, 2).items()}
+    keys = [KW, KU]
+    w = {k: torch.tensor(p[k], dtype=torch.float64, device=DEV, requires_grad=True) for k in keys}
+    roll = ClosedLoopRollout(solver, num_sim_steps=20, simulator="model", state_weight=10.0)
+    cost = roll(torch.tensor(x0s, device=DEV), bp, w)
+    loss = -cost.sum()
+    loss.backward()
+    want = -2.8196995973193135
+    assert abs(float(loss) - want) < (1e-10 if precision == "fp64" else 1e-6) * abs(want)
+    new_u = torch.clamp(w[KU] + w[KU].grad, min=1e-10).detach().cpu().numpy()
+    new_x = torch.clamp(w[KW] + w[KW].grad, min=1e-10).detach().cpu().numpy()
+    assert np.allclose(new_u, [0.9955808, 0.9085766, 0.8319815], atol=5e-5)
+    assert np.allclose(new_x, [1.0033015, 1.09093417, 1.16958629], atol=5e-5)
