@@ -576,7 +576,7 @@ def run_other_workload(args):
         solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp, device=dev)
         p = workloads.to_device(bt, dev)
         keys = ["weights_penalization_reference_state_trajectory", "weights_penalization_control_squared"]
-        roll = ClosedLoopRollout(solver, num_sim_steps=T, simulator="model", state_weight=10.0)
+        roll = ClosedLoopRollout(solver, num_sim_steps=T, simulator="euler", state_weight=10.0)
 
         def run(grad):
             w = {k: p[k].clone().requires_grad_(grad) for k in keys}

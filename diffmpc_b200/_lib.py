@@ -22,7 +22,7 @@ DMPC_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 MODEL_IDS = {"linear": 0, "quadrotor": 1, "spacecraft": 2, "attitude": 3, "cartpole": 4}
 PREC_FP64, PREC_MIXED = 0, 1
-SIM_LINEAR, SIM_MODEL = 0, 1
+SIM_LINEAR, SIM_MODEL, SIM_MODEL_SCHEME = 0, 1, 2
 
 EXPORTED_SYMBOLS = (
     "dmpc_abi_version",
@@ -130,8 +130,10 @@ class Rollout(ctypes.Structure):
         ("warm_start", _i32),
         ("simulator", _i32),
         ("reserved", _i32),
-        ("cost_state_weight", _f64),
-        ("cost_control_weight", _f64),
+        ("cost_state_weights", _p),
+        ("cost_control_weights", _p),
+        ("cost_state_ref", _p),
+        ("cost_control_ref", _p),
         ("sim_A", _p),
         ("sim_B", _p),
         ("sim_b", _p),

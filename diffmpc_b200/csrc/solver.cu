@@ -1308,9 +1308,9 @@ __global__ void __launch_bounds__(512, 1) k_sqp_fwd(const __grid_constant__ DevA
 }
 
 // ---------------------------------------------------------------- closed-loop rollout
-// One Euler step of the instance's model as the rollout's simulator: sum_i lam_i d(x+_i)/dz_d
+// One integrator step of the instance's model as the rollout's simulator (s.scheme: Euler
+// for DMPC_SIM_MODEL, the group's scheme for DMPC_SIM_MODEL_SCHEME): sum_i lam_i d(x+_i)/dz_d
 // for the direction z_d of (x, u) (d < nx: state, else control), by one Dual evaluation.
-// `s` must carry scheme DMPC_EULER.
 template <int MODEL>
 __device__ __noinline__ double sim_vjp_item(const Inst& s, const double* x, const double* u, const double* lam, int d) {
   constexpr int MX = ModelDims<MODEL>::NX, MU = ModelDims<MODEL>::NU;
@@ -1324,7 +1324,7 @@ __device__ __noinline__ double sim_vjp_item(const Inst& s, const double* x, cons
     Dual p[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) p[k] = Dual(k < s.P ? s.mp[k] : 0.0);
-    predict_next_state<Dual, MODEL>(DMPC_EULER, s.dt, nx, nu, xd, ud, p, xn);
+    predict_next_state<Dual, MODEL>(s.scheme, s.dt, nx, nu, xd, ud, p, xn);
   }
   double acc = 0.0;
   for (int i = 0; i < nx; ++i) acc += lam[i] * xn[i].d;
@@ -1366,8 +1366,9 @@ __device__ inline dmpc_group rollout_step_view(const dmpc_group& g0, const dmpc_
 // benchmark_diffmpc.py:140-175 (lax.scan of rollout_step, vmapped over instances), one CTA
 // per instance for all simulation steps: solve the MPC from x_k (warm-started from step
 // k-1's solution, or from the initial guess), apply u_k = controls[0], simulate x_{k+1}
-// (x_{k+1} = A x_k + B u_k + b, or an Euler step of the model as in
-// spacecraft/benchmark_diffmpc.py:87-89) and add ws |x_{k+1}|^2 + wc |u_k|^2.  Every
+// (x_{k+1} = A x_k + B u_k + b, or an integrator step of the model as in
+// spacecraft/benchmark_diffmpc.py:87-89) and add the weighted squared deviations of x_{k+1}
+// and u_k.  Every
 // step's solution and last linearization point are kept for the adjoint sweep.
 __global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ DevArgs args,
                                                         const __grid_constant__ dmpc_rollout ra, void* ws) {
@@ -1415,10 +1416,10 @@ __global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ 
     const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
     const double* u = sh_g.controls + ou;  // controls[0]
     double* xn = ra.step_initial_state + ((size_t)(k + 1) * B + ii) * nx;
-    if (ra.simulator == DMPC_SIM_MODEL) {
+    if (ra.simulator != DMPC_SIM_LINEAR) {
       if (threadIdx.x == 0) {
         Inst se = make_inst(G, sh_g, ii, ws, nullptr);
-        se.scheme = DMPC_EULER;
+        if (ra.simulator == DMPC_SIM_MODEL) se.scheme = DMPC_EULER;
         next_state_value(se, x, u, xn);
       }
     } else {
@@ -1433,10 +1434,16 @@ __global__ void __launch_bounds__(512, 1) k_rollout_fwd(const __grid_constant__ 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      double cx = 0.0, cu = 0.0;
-      for (int i = 0; i < nx; ++i) cx += xn[i] * xn[i];
-      for (int j = 0; j < nu; ++j) cu += u[j] * u[j];
-      sh_cost += ra.cost_state_weight * cx + ra.cost_control_weight * cu;
+      double c = 0.0;
+      for (int i = 0; i < nx; ++i) {
+        const double d = xn[i] - (ra.cost_state_ref ? ra.cost_state_ref[i] : 0.0);
+        c += ra.cost_state_weights[i] * d * d;
+      }
+      for (int j = 0; j < nu; ++j) {
+        const double d = u[j] - (ra.cost_control_ref ? ra.cost_control_ref[j] : 0.0);
+        c += ra.cost_control_weights[j] * d * d;
+      }
+      sh_cost += c;
     }
     __syncthreads();
   }
@@ -1576,10 +1583,10 @@ __global__ void __launch_bounds__(512, 1) k_sqp_adj(const __grid_constant__ DevA
 }
 
 // Reverse sweep of the rollout's gradient (what jax.grad of the reference's scan computes):
-// with lam_T = 2 c ws x_T (c = dL/d running cost), F the simulator step, for k = T-1 .. 0
-//   dl/du_0 of step k  = 2 c wc u_k + (dF/du)^T lam_{k+1}
+// with lam_T = c dcost/dx_T (c = dL/d running cost), F the simulator step, for k = T-1 .. 0
+//   dl/du_0 of step k  = c dcost/du_k + (dF/du)^T lam_{k+1}
 //   adjoint of step k's solve, parameter gradients accumulated into adj's outputs
-//   lam_k = (dF/dx)^T lam_{k+1} + 2 c ws x_k (k >= 1) [+ the solve's dL/dx_0 if through_state]
+//   lam_k = (dF/dx)^T lam_{k+1} + c dcost/dx_k (k >= 1) [+ the solve's dL/dx_0 if through_state]
 // (dF/dz)^T lam is formed by one Dual evaluation per direction for the model simulator.
 // and dL/dx_0 = lam_0.  One CTA per instance, all steps in one launch.
 __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ DevArgs args,
@@ -1597,9 +1604,15 @@ __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ 
   __shared__ dmpc_adjoint sh_a;
   __shared__ double sh_lam[DMPC_MAX_NX], sh_vjp[DMPC_MAX_NX + DMPC_MAX_NU];
   const double c = rr.cost_cotangent[ii];
-  const double cs = 2.0 * c * ra.cost_state_weight, cc = 2.0 * c * ra.cost_control_weight;
   const int T = ra.num_steps;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = cs * ra.step_initial_state[((size_t)T * B + ii) * nx + i];
+  // d cost / dx_k and d cost / du_k of the running cost's terms
+  auto dcx = [&](const double* x, int i) {
+    return 2.0 * c * ra.cost_state_weights[i] * (x[i] - (ra.cost_state_ref ? ra.cost_state_ref[i] : 0.0));
+  };
+  auto dcu = [&](const double* u, int j) {
+    return 2.0 * c * ra.cost_control_weights[j] * (u[j] - (ra.cost_control_ref ? ra.cost_control_ref[j] : 0.0));
+  };
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) sh_lam[i] = dcx(ra.step_initial_state + ((size_t)T * B + ii) * nx, i);
   for (int w = threadIdx.x; w < Kmax * nu; w += blockDim.x) rr.scratch_dl_dcontrols[ou + w] = 0.0;
   __syncthreads();
   for (int k = T - 1; k >= 0; --k) {
@@ -1620,10 +1633,10 @@ __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ 
     const double* u = sh_g.controls + ou;  // u_k = controls[0]
     const double* x = ra.step_initial_state + ((size_t)k * B + ii) * nx;
     // sh_vjp = [dx_{k+1}/dx_k, dx_{k+1}/du_k]^T lam_{k+1}
-    if (ra.simulator == DMPC_SIM_MODEL) {
+    if (ra.simulator != DMPC_SIM_LINEAR) {
       for (int d = threadIdx.x; d < nx + nu; d += blockDim.x) {
         Inst se = make_inst(G, sh_g, ii, ws, nullptr);
-        se.scheme = DMPC_EULER;
+        if (ra.simulator == DMPC_SIM_MODEL) se.scheme = DMPC_EULER;
         sh_vjp[d] = sim_vjp(se, x, u, sh_lam, d);
       }
     } else {
@@ -1639,14 +1652,14 @@ __global__ void __launch_bounds__(512, 1) k_rollout_adj(const __grid_constant__ 
       }
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < nu; j += blockDim.x) rr.scratch_dl_dcontrols[ou + j] = cc * u[j] + sh_vjp[nx + j];
+    for (int j = threadIdx.x; j < nu; j += blockDim.x) rr.scratch_dl_dcontrols[ou + j] = dcu(u, j) + sh_vjp[nx + j];
     __syncthreads();
     sqp_adjoint(G, sh_g, sh_a, ii, args.p, ws, smem, true);
     __syncthreads();
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
       double v = sh_vjp[i];
       if (rr.through_state) v += rr.scratch_dual[ox + i];  // the solve's dL/dx_0 = lam~_0
-      if (k >= 1) v += cs * x[i];
+      if (k >= 1) v += dcx(x, i);
       sh_lam[i] = v;
     }
     __syncthreads();
@@ -2235,7 +2248,8 @@ int dmpc_rollout_adj(const dmpc_group* group, const dmpc_rollout* ro, const dmpc
                      const dmpc_rollout_adjoint* rr, const dmpc_solver_params* params, void* workspace,
                      size_t workspace_bytes, void* stream) {
   if (!group || !ro || !adj || !rr || ro->num_steps < 1) return DMPC_ERR_INVALID;
-  if (ro->simulator != DMPC_SIM_LINEAR && ro->simulator != DMPC_SIM_MODEL) return DMPC_ERR_INVALID;
+  if (ro->simulator < DMPC_SIM_LINEAR || ro->simulator > DMPC_SIM_MODEL_SCHEME) return DMPC_ERR_INVALID;
+  if (!ro->cost_state_weights || !ro->cost_control_weights) return DMPC_ERR_INVALID;
   if (ro->simulator == DMPC_SIM_LINEAR && (!ro->sim_A || !ro->sim_B)) return DMPC_ERR_INVALID;
   if (!ro->step_initial_state || !ro->step_states || !ro->step_controls ||
       !ro->step_dual || !ro->step_lin_states || !ro->step_lin_controls || !ro->step_status || !ro->step_num_iter ||
@@ -2263,7 +2277,8 @@ int dmpc_rollout_adj(const dmpc_group* group, const dmpc_rollout* ro, const dmpc
 int dmpc_rollout_fwd(const dmpc_group* group, const dmpc_rollout* ro, const dmpc_solver_params* params,
                      void* workspace, size_t workspace_bytes, void* stream) {
   if (!group || !ro || ro->num_steps < 1) return DMPC_ERR_INVALID;
-  if (ro->simulator != DMPC_SIM_LINEAR && ro->simulator != DMPC_SIM_MODEL) return DMPC_ERR_INVALID;
+  if (ro->simulator < DMPC_SIM_LINEAR || ro->simulator > DMPC_SIM_MODEL_SCHEME) return DMPC_ERR_INVALID;
+  if (!ro->cost_state_weights || !ro->cost_control_weights) return DMPC_ERR_INVALID;
   if (ro->simulator == DMPC_SIM_LINEAR && (!ro->sim_A || !ro->sim_B || !ro->sim_b)) return DMPC_ERR_INVALID;
   if (!ro->step_initial_state || !ro->step_states || !ro->step_controls ||
       !ro->step_dual || !ro->step_lin_states || !ro->step_lin_controls || !ro->step_status || !ro->step_num_iter ||

@@ -59,6 +59,10 @@ class _RolloutFunction(torch.autograd.Function):
         f64 = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)  # noqa: E731
         i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
         linear = roll.simulator == "linear"
+        vec = lambda v, n: torch.as_tensor(v, dtype=torch.float64, device=dev).expand(n).contiguous()  # noqa: E731
+        cw = SimpleNamespace(ws=vec(roll.state_weight, nx), wc=vec(roll.control_weight, nu),
+                             xr=None if roll.state_ref is None else vec(roll.state_ref, nx),
+                             ur=None if roll.control_ref is None else vec(roll.control_ref, nu))
         st = SimpleNamespace(
             A=_per_instance(roll.sim_A, B, (nx, nx), dev) if linear else None,
             Bm=_per_instance(roll.sim_B, B, (nx, nu), dev) if linear else None,
@@ -69,8 +73,10 @@ class _RolloutFunction(torch.autograd.Function):
         )
         r = _lib.Rollout()
         r.num_steps, r.warm_start = T, 1 if roll.warm_start else 0
-        r.simulator = _lib.SIM_LINEAR if linear else _lib.SIM_MODEL
-        r.cost_state_weight, r.cost_control_weight = roll.state_weight, roll.control_weight
+        r.simulator = {"linear": _lib.SIM_LINEAR, "euler": _lib.SIM_MODEL, "integrator": _lib.SIM_MODEL_SCHEME}[
+            roll.simulator]
+        r.cost_state_weights, r.cost_control_weights = _ptr(cw.ws), _ptr(cw.wc)
+        r.cost_state_ref, r.cost_control_ref = _ptr(cw.xr), _ptr(cw.ur)
         r.sim_A, r.sim_B, r.sim_b = _ptr(st.A), _ptr(st.Bm), _ptr(st.b)
         r.step_initial_state, r.step_states, r.step_controls = _ptr(st.x), _ptr(st.states), _ptr(st.controls)
         r.step_dual, r.step_lin_states, r.step_lin_controls = _ptr(st.dual), _ptr(st.lin_states), _ptr(st.lin_controls)
@@ -88,7 +94,7 @@ class _RolloutFunction(torch.autograd.Function):
                    "dmpc_rollout_fwd")
         solver._event_end(ev, "k_rollout_fwd")
         roll.last = st
-        ctx.roll, ctx.call, ctx.st, ctx.keys, ctx.r = roll, call, st, keys, r
+        ctx.roll, ctx.call, ctx.st, ctx.keys, ctx.r, ctx.cw = roll, call, st, keys, r, cw
         ctx.shapes = [v.shape for v in vals]
         return st.cost.clone()
 
@@ -144,13 +150,15 @@ def _per_step_sweep(ctx, g_cost):
     solver = roll.solver
     B, K, nx, nu, T = call.B, call.K, call.nx, call.nu, roll.num_sim_steps
     go = g_cost.to(torch.float64).reshape(B, 1)
-    ws_, wc_ = roll.state_weight, roll.control_weight
+    cw = ctx.cw
+    dcx = lambda x: 2.0 * go * cw.ws * (x - (0.0 if cw.xr is None else cw.xr))  # noqa: E731
+    dcu = lambda u: 2.0 * go * cw.wc * (u - (0.0 if cw.ur is None else cw.ur))  # noqa: E731
     akeys = list(keys) + (["initial_state"] if roll.through_state and "initial_state" not in keys else [])
     acc = {}
-    lam = 2.0 * ws_ * go * st.x[T]
+    lam = dcx(st.x[T])
     for k in reversed(range(T)):
         u = st.controls[k, :, 0]
-        g_u = 2.0 * wc_ * go * u + torch.einsum("bij,bi->bj", st.Bm, lam)
+        g_u = dcu(u) + torch.einsum("bij,bi->bj", st.Bm, lam)
         dlu = torch.zeros(B, K, nu, dtype=torch.float64, device=u.device)
         dlu[:, 0] = g_u
         g = _lib.Group.from_buffer_copy(call.group)
@@ -169,7 +177,7 @@ def _per_step_sweep(ctx, g_cost):
         if roll.through_state:
             lam = lam + grads["initial_state"]
         if k >= 1:
-            lam = lam + 2.0 * ws_ * go * st.x[k]
+            lam = lam + dcx(st.x[k])
     return acc, lam
 
 
@@ -177,17 +185,20 @@ class ClosedLoopRollout:
     """MPC-in-the-loop rollout of ``num_sim_steps`` steps.
 
     ``simulator="linear"``: ``x+ = sim_A x + sim_B u + sim_b`` (each shared by the batch or
-    given per instance), as in benchmark_diffmpc.py:148-150.  ``simulator="model"``: one
-    Euler step ``x+ = x + dt f(x, u)`` of the solver's own model with each instance's ``dt``
-    and model parameters, as in spacecraft/benchmark_diffmpc.py:87-89.  The simulator uses
-    the model parameters the solves see (a weight that overrides one applies to both) and is
-    not differentiated with respect to them.
+    given per instance), as in benchmark_diffmpc.py:148-150.  ``simulator="euler"``: one Euler
+    step ``x+ = x + dt f(x, u)`` of the solver's own model with each instance's ``dt`` and
+    model parameters, as in spacecraft/benchmark_diffmpc.py:87-89.  ``simulator="integrator"``:
+    one step of the solver's own integrator (its discretization scheme), as the RL_quadrotor
+    notebook simulates.  The model simulators use the model parameters the solves see (a
+    weight that overrides one applies to both) and are not differentiated with respect to them.
 
     ``rollout(initial_states, problem_params, weights)`` returns the running cost
-    ``sum_k state_weight |x_{k+1}|^2 + control_weight |u_k|^2`` per instance (shape ``(B,)``;
-    the reference scripts' reward is its negative, with weights 1, 1 for the linear and
-    10, 1 for the spacecraft benchmark), differentiable with respect to ``weights`` (any key
-    ``SQPSolver.solve`` accepts) and ``initial_states``.
+    ``sum_k sum_i state_weight_i (x_{k+1,i} - state_ref_i)^2 + sum_j control_weight_j
+    (u_{k,j} - control_ref_j)^2`` per instance (shape ``(B,)``; weights are scalars or
+    vectors shared by the batch, references default to zero).  The reference scripts' reward
+    is its negative: weights 1, 1 for the linear benchmark, 10, 1 for the spacecraft one.  It
+    is differentiable with respect to ``weights`` (any key ``SQPSolver.solve`` accepts) and
+    ``initial_states``.
     ``warm_start`` starts each solve from the previous step's solution, as the
     reference's ``warm_start`` flag does.  The backward pass is one launch per parameter
     chunk (``dmpc_rollout_adj``); for the linear simulator ``fused_backward=False`` runs
@@ -197,15 +208,16 @@ class ClosedLoopRollout:
 
     def __init__(self, solver: SQPSolver, sim_A=None, sim_B=None, sim_b=None, num_sim_steps: int = 1,
                  warm_start: bool = True, through_state: bool = False, fused_backward: bool = True,
-                 simulator: str = "linear", state_weight: float = 1.0, control_weight: float = 1.0):
+                 simulator: str = "linear", state_weight=1.0, control_weight=1.0, state_ref=None, control_ref=None):
         if num_sim_steps < 1:
             raise ValueError("num_sim_steps must be >= 1")
-        if simulator not in ("linear", "model"):
-            raise ValueError("simulator must be 'linear' or 'model'")
+        if simulator not in ("linear", "euler", "integrator"):
+            raise ValueError("simulator must be 'linear', 'euler' or 'integrator'")
         if simulator == "linear" and (sim_A is None or sim_B is None or sim_b is None):
             raise ValueError("the linear simulator needs sim_A, sim_B and sim_b")
         self.simulator = simulator
-        self.state_weight, self.control_weight = float(state_weight), float(control_weight)
+        self.state_weight, self.control_weight = state_weight, control_weight
+        self.state_ref, self.control_ref = state_ref, control_ref
         self.solver = solver
         self.sim_A, self.sim_B, self.sim_b = sim_A, sim_B, sim_b
         self.num_sim_steps = int(num_sim_steps)

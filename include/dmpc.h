@@ -165,19 +165,26 @@ typedef struct dmpc_adjoint {
  * rollout_step scanned with lax.scan and vmapped over instances).  For k = 0..num_steps-1:
  * solve the MPC with initial state x_k starting from step k-1's solution (warm_start) or from
  * the group's initial guess, apply u_k = controls[0], simulate x_{k+1} (see `simulator`) and add
- * cost_state_weight |x_{k+1}|^2 + cost_control_weight |u_k|^2 to the running cost (the reference
- * scripts' negated reward: weights 1, 1 for the linear benchmark, 10, 1 for the spacecraft one).  All pointers are device memory; K = horizon+1,
+ * the weighted squared deviations of x_{k+1} and u_k to the running cost (the reference scripts'
+ * negated reward: |x|^2 + |u|^2 for the linear benchmark, 10 |x|^2 + |u|^2 for the spacecraft
+ * one, |p - p_ref|^2 + 0.1 |u - u_ref|^2 for the RL_quadrotor notebook).  All pointers are device memory; K = horizon+1,
  * T = num_steps. */
 #define DMPC_SIM_LINEAR 0 /* x+ = A x + B u + b (benchmark_diffmpc.py:148-150) */
 #define DMPC_SIM_MODEL 1  /* x+ = x + dt f(x, u): one Euler step of the group's model with each instance's
                              dt and model parameters (spacecraft/benchmark_diffmpc.py:87-89) */
+#define DMPC_SIM_MODEL_SCHEME 2 /* one step of the group's own integrator (its discretization scheme),
+                                   as the RL_quadrotor notebook simulates (cell 12) */
 typedef struct {
   int32_t num_steps;                /* T >= 1 */
   int32_t warm_start;               /* 1: step k starts from step k-1's solution */
-  int32_t simulator;                /* DMPC_SIM_LINEAR or DMPC_SIM_MODEL */
+  int32_t simulator;                /* DMPC_SIM_LINEAR, DMPC_SIM_MODEL or DMPC_SIM_MODEL_SCHEME */
   int32_t reserved;                 /* 0 */
-  double cost_state_weight;         /* running cost += cost_state_weight |x_{k+1}|^2 */
-  double cost_control_weight;       /*               + cost_control_weight |u_k|^2 */
+  /* running cost += sum_i ws_i (x_{k+1,i} - xr_i)^2 + sum_j wc_j (u_{k,j} - ur_j)^2; all four
+   * arrays are shared by the batch, and a null reference is zero */
+  const double* cost_state_weights;   /* (nx) */
+  const double* cost_control_weights; /* (nu) */
+  const double* cost_state_ref;       /* (nx) or null */
+  const double* cost_control_ref;     /* (nu) or null */
   const double* sim_A;              /* (batch, nx, nx) DMPC_SIM_LINEAR only */
   const double* sim_B;              /* (batch, nx, nu) DMPC_SIM_LINEAR only */
   const double* sim_b;              /* (batch, nx)     DMPC_SIM_LINEAR only */

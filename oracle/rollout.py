@@ -15,6 +15,8 @@ instead, which differentiates through the solve's dependence on it.
 import torch
 from torch.func import vmap
 
+from oracle.ocp import EULER, predict_next_state
+
 
 def _stop(sol):
     return sol._replace(
@@ -23,24 +25,26 @@ def _stop(sol):
     )
 
 
-def _model_step(solver, problem_params, x, u):
-    """``x + dt f(x, u)`` with the solver's model and each instance's parameters
-    (spacecraft/benchmark_diffmpc.py:87-89)."""
+def _model_step(solver, problem_params, x, u, scheme=EULER):
+    """One step of the solver's model with each instance's dt and parameters: Euler as in
+    spacecraft/benchmark_diffmpc.py:87-89, or the program's own scheme (RL_quadrotor)."""
     model = solver.program.model
     p = {k: problem_params[k] for k in model.param_keys}
-    f = vmap(model.state_dot)(x, u, p)
-    dt = torch.as_tensor(problem_params["discretization_resolution"], dtype=torch.float64).reshape(-1, 1)
-    return x + dt * f
+    dt = torch.as_tensor(problem_params["discretization_resolution"], dtype=torch.float64).reshape(-1)
+    return vmap(lambda xx, uu, pp, h: predict_next_state(model, h, scheme, pp, xx, uu))(x, u, p, dt)
 
 
 def rollout(solver, problem_params, initial_states, weights, A, Bm, b, num_steps, warm_start=True,
-            through_state=False, simulator="linear", state_weight=1.0, control_weight=1.0):
+            through_state=False, simulator="linear", state_weight=1.0, control_weight=1.0, state_ref=0.0,
+            control_ref=0.0, initial_guess=None):
     """Returns (running cost (B,), [u_k], [x_k]); differentiable w.r.t. ``weights``.
-    ``simulator="model"`` replaces ``A x + B u + b`` by an Euler step of the solver's model
-    (A, Bm, b unused); the cost is state_weight |x_{k+1}|^2 + control_weight |u_k|^2 (the
-    spacecraft script's reward is -(10 |x|^2 + |u|^2), spacecraft/utils.py)."""
+    ``simulator="euler"`` / ``"integrator"`` replace ``A x + B u + b`` by an Euler step / a step
+    of the program's own integrator (A, Bm, b unused).  The cost is
+    sum state_weight (x_{k+1} - state_ref)^2 + control_weight (u_k - control_ref)^2 (scalars or
+    vectors); the spacecraft script's reward is -(10 |x|^2 + |u|^2), spacecraft/utils.py."""
     x = initial_states
-    guess0 = solver.initial_guess({**problem_params, "initial_state": x.detach()})
+    guess0 = initial_guess if initial_guess is not None else \
+        solver.initial_guess({**problem_params, "initial_state": x.detach()})
     guess = guess0
     cost = torch.zeros(x.shape[0], dtype=torch.float64)
     us, xs = [], [x]
@@ -50,12 +54,15 @@ def rollout(solver, problem_params, initial_states, weights, A, Bm, b, num_steps
         else:
             sol = solver.solve(guess, {**problem_params, "initial_state": x.detach()}, weights)
         u = sol.controls[:, 0]
-        if simulator == "model":
+        if simulator in ("euler", "integrator"):
             # the model parameters as the solve sees them, not differentiated through the simulator
-            x_new = _model_step(solver, {**problem_params, **{k: v.detach() for k, v in weights.items()}}, x, u)
+            scheme = EULER if simulator == "euler" else solver.program.scheme
+            x_new = _model_step(solver, {**problem_params, **{k: v.detach() for k, v in weights.items()}}, x, u, scheme)
         else:
             x_new = torch.einsum("bij,bj->bi", A, x) + torch.einsum("bij,bj->bi", Bm, u) + b
-        cost = cost + state_weight * (x_new ** 2).sum(-1) + control_weight * (u ** 2).sum(-1)
+        ws, wc = torch.as_tensor(state_weight, dtype=torch.float64), torch.as_tensor(control_weight, dtype=torch.float64)
+        xr, ur = torch.as_tensor(state_ref, dtype=torch.float64), torch.as_tensor(control_ref, dtype=torch.float64)
+        cost = cost + (ws * (x_new - xr) ** 2).sum(-1) + (wc * (u - ur) ** 2).sum(-1)
         guess = _stop(sol) if warm_start else guess0
         x = x_new
         us.append(u)

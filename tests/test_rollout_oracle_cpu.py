@@ -80,7 +80,7 @@ def test_oracle_model_simulator_rollout_gradient_matches_finite_differences(thro
     keys = ["weights_penalization_control_squared", KEY]
     w = {k: p[k].clone().requires_grad_(True) for k in keys}
     x0 = p["initial_state"]
-    kw = dict(warm_start=True, simulator="model", state_weight=10.0)
+    kw = dict(warm_start=True, simulator="euler", state_weight=10.0)
     cost, _, xs = rollout(solver, p, x0, w, None, None, None, T, through_state=through_state, **kw)
     grads = torch.autograd.grad(cost.sum(), [w[k] for k in keys])
     xs_nominal = [x.detach() for x in xs]
