@@ -94,13 +94,16 @@ typedef struct dmpc_solver_params {
   int32_t n_alphas;               /* len(linesearch_alphas) <= DMPC_MAX_ALPHAS */
   double alphas[DMPC_MAX_ALPHAS]; /* sqp.yaml linesearch_alphas */
   int32_t warm_start_backward;    /* sqp.yaml warm_start_backward */
-  int32_t pcg_max_iter;           /* sqp.yaml pcg.max_iter */
+  int32_t pcg_max_iter;           /* sqp.yaml pcg.max_iter.  MIXED: FP32 iterations use at most half of it;
+                                     an FP64 fallback recurrence then gets a full budget of its own */
   double pcg_tol_epsilon;         /* sqp.yaml pcg.tol_epsilon (absolute, on eta = r^T Phi^-1 r) */
   int32_t precision;              /* DMPC_PREC_* */
   int32_t max_refinement;         /* MIXED: outer FP64 refinement steps per QP solve */
   double inner_rel_tol;           /* MIXED: inner FP32 PCG stops when eta32 <= inner_rel_tol * eta at restart */
-  int32_t threads_per_block;      /* 0 = automatic (autotuned table) */
-  int32_t blocks_in_smem;         /* -1 auto, 0 force global-memory blocks, 1 require shared memory */
+  int32_t threads_per_block;      /* 0 = automatic: one thread per row pair of the FP32 PCG (else per row),
+                                     256..512; or 64..512, a multiple of 32 (diffmpc_b200.autotune) */
+  int32_t blocks_in_smem;         /* MIXED, the FP32 scaled off-diagonal blocks: -1 shared memory when they
+                                     fit (per instance in a ragged group), 0 workspace, 1 require shared */
 } dmpc_solver_params;
 
 /* One group = instances sharing model, nx, nu and max horizon (a batch).
