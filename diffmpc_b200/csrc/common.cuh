@@ -125,30 +125,36 @@ __device__ inline bool warp_chol_inverse(double* A, double* X, int n) {
   return ok;
 }
 
-// Register-resident variant for compile-time NX <= 16: ONE warp factors the SPD block
-// th (NX x NX, row-major) as L L^T and writes X = L^-1 to li (row-major, zeros above the
-// diagonal).  Lane i holds row i of the block, then of L, in registers; the forward
-// substitution gives lane c column c of X.  Every operand crosses lanes by shuffle, so the
-// only memory traffic is one read of th and one coalesced write of X.  Lanes >= NX mirror
-// row 0 and store nothing.  Returns false in every lane if a pivot is not positive and
-// finite.
-template <int NX>
-__device__ __forceinline__ bool warp_chol_inverse_regs(const double* __restrict__ th, double* __restrict__ li) {
-  const int lane = threadIdx.x & 31;
+// Register-resident variant for compile-time NX: a group of W lanes (W = 16 for NX <= 16,
+// else 32; a warp holds 32 / W groups, each on its own block) factors the SPD block th
+// (NX x NX, row-major) as L L^T and writes X = L^-1 to li (row-major, zeros above the
+// diagonal).  Lane i of the group holds row i of the block, then of L, in registers; the
+// forward substitution gives lane c column c of X.  Operands cross lanes by width-W
+// shuffles, so the only memory traffic is one read of th and one coalesced write of X.
+// Each pivot's reciprocal is formed once and reused by the substitution.  Lanes >= NX
+// mirror row 0, and a group with `active` false (no block left for it) computes on th
+// without storing; all lanes of the warp must call this together.  Returns false if a
+// pivot of an active group is not positive and finite.
+template <int NX, int W>
+__device__ __forceinline__ bool group_chol_inverse_regs(const double* __restrict__ th, double* __restrict__ li,
+                                                        bool active) {
+  static_assert(NX <= W && (W == 16 || W == 32), "one lane per row");
+  const int lane = threadIdx.x & (W - 1);
   const int r = lane < NX ? lane : 0;
-  double a[NX];
+  double a[NX], rd[NX];
 #pragma unroll
   for (int j = 0; j < NX; ++j) a[j] = th[r * NX + j];
   bool ok = true;
 #pragma unroll
   for (int k = 0; k < NX; ++k) {
-    const double piv = __shfl_sync(DMPC_FULL_MASK, a[k], k);
+    const double piv = __shfl_sync(DMPC_FULL_MASK, a[k], k, W);
     ok = ok && piv > 0.0 && isfinite(piv);
     const double d = sqrt(piv);
-    a[k] = (lane == k) ? d : a[k] / d;  // lanes > k: L[lane][k]; lanes < k keep a finished row
+    rd[k] = 1.0 / d;
+    a[k] = (lane == k) ? d : a[k] * rd[k];  // lanes > k: L[lane][k]; lanes < k keep a finished row
 #pragma unroll
     for (int j = k + 1; j < NX; ++j) {
-      const double ljk = __shfl_sync(DMPC_FULL_MASK, a[k], j);
+      const double ljk = __shfl_sync(DMPC_FULL_MASK, a[k], j, W);
       if (lane >= j) a[j] = fma(-a[k], ljk, a[j]);
     }
   }
@@ -158,12 +164,12 @@ __device__ __forceinline__ bool warp_chol_inverse_regs(const double* __restrict_
   for (int i = 0; i < NX; ++i) {
     double acc = (lane == i) ? 1.0 : 0.0;
 #pragma unroll
-    for (int k = 0; k < i; ++k) acc = fma(-__shfl_sync(DMPC_FULL_MASK, a[k], i), x[k], acc);
-    x[i] = acc / __shfl_sync(DMPC_FULL_MASK, a[i], i);
+    for (int k = 0; k < i; ++k) acc = fma(-__shfl_sync(DMPC_FULL_MASK, a[k], i, W), x[k], acc);
+    x[i] = acc * rd[i];
   }
-  if (lane < NX) {
+  if (active && lane < NX) {
 #pragma unroll
     for (int i = 0; i < NX; ++i) li[i * NX + lane] = x[i];
   }
-  return ok;
+  return ok || !active;
 }

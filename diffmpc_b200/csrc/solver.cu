@@ -366,15 +366,23 @@ __device__ void linearize_cost(const Inst& s, const double* xb, const double* ub
 // FP64 recurrence instead of the scaled FP32 iterations.
 __shared__ int sh_scaled_bad;
 
-// Li_t = L_t^-1 for every knot (theta_t = L_t L_t^T, FP64), one warp per block: in
-// registers for the nx with a row-pair PCG, else in the workspace (tmp as the
+// Li_t = L_t^-1 for every knot (theta_t = L_t L_t^T, FP64): in registers by groups of 16
+// lanes per block for the nx with a row-pair PCG, else one warp per block in the workspace (tmp as the
 // factorisation's working copy).  Sets sh_scaled_bad if a block has no factor.
 template <int NX>
 __device__ __noinline__ bool scaled_factors_regs(const Inst& s) {
   constexpr int nn = NX * NX;
+  constexpr int W = NX <= 16 ? 16 : 32;  // lanes per block
+  constexpr int G = 32 / W;              // blocks per warp at a time
+  const int gid = (threadIdx.x >> 5) * G + ((threadIdx.x & 31) / W);
+  const int ng = (blockDim.x >> 5) * G;
   bool ok = true;
-  for (int t = threadIdx.x >> 5; t < s.K; t += blockDim.x >> 5)
-    ok = warp_chol_inverse_regs<NX>(s.th + (size_t)t * nn, s.li + (size_t)t * nn) && ok;
+  for (int base = 0; base < s.K; base += ng) {  // warp-uniform rounds
+    const int t = base + gid;
+    const bool active = t < s.K;
+    const size_t o = (size_t)(active ? t : 0) * nn;
+    ok = group_chol_inverse_regs<NX, W>(s.th + o, s.li + o, active) && ok;
+  }
   return ok;
 }
 
