@@ -449,46 +449,53 @@ __device__ __noinline__ void assemble_schur_t(const Inst& s, bool fp32_copy) {
   if (!fp32_copy) {
     for (int t = warp; t < K; t += nwarp) warp_spd_inverse(s.tmp + (size_t)t * nn, s.ti + (size_t)t * nn, nx);
   } else {
-    // Li_t = L_t^-1 with theta_t = L_t L_t^T, then theta_t^-1 = Li_t^T Li_t
+    // Li_t = L_t^-1 with theta_t = L_t L_t^T.  The mixed path needs no theta^-1 or P: its
+    // FP64 residual and fallback work in the scaled basis.  Without a factor (a theta block
+    // that is not numerically SPD) it falls back to the reference recurrence, which needs them.
     scaled_factors(s);
     __syncthreads();
-    for (int w = threadIdx.x; w < K * nn; w += blockDim.x) {
-      const int t = w / nn, e = w - t * nn, a = e / nx, b = e - a * nx;
-      const double* X = s.li + (size_t)t * nn;
-      double acc = 0.0;
-#pragma unroll
-      for (int k = 0; k < nx; ++k) acc += X[k * nx + a] * X[k * nx + b];  // X is zero above the diagonal
-      s.ti[w] = acc;
+    if (sh_scaled_bad) {
+      for (int t = warp; t < K; t += nwarp) {
+        double* Lt = s.tmp + (size_t)t * nn;
+        for (int e = (threadIdx.x & 31); e < nn; e += 32) Lt[e] = s.th[(size_t)t * nn + e];
+        __syncwarp();
+        warp_spd_inverse(Lt, s.ti + (size_t)t * nn, nx);
+      }
     }
   }
   __syncthreads();
-  // T_t = theta_t^-1 phi_{t-1}  (t = 1..N), stored in tmp block t
-  for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
-    const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
-    const int t = k + 1;
-    const double* Ti = s.ti + (size_t)t * nn + i * nx;
-    const double* Pk = s.ph + (size_t)k * nn + j;
-    double a = 0.0;
+  // reference-basis Phi^-1 blocks (pcg.py:213-239): the FP64 path, or the mixed path without
+  // Cholesky factors
+  if (!fp32_copy || sh_scaled_bad) {
+    // T_t = theta_t^-1 phi_{t-1}  (t = 1..N), stored in tmp block t
+    for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
+      const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
+      const int t = k + 1;
+      const double* Ti = s.ti + (size_t)t * nn + i * nx;
+      const double* Pk = s.ph + (size_t)k * nn + j;
+      double a = 0.0;
 #pragma unroll
-    for (int l = 0; l < nx; ++l) a += Ti[l] * Pk[l * nx];
-    s.tmp[(size_t)t * nn + e] = a;
-  }
-  __syncthreads();
-  // P_t = -T_t theta_{t-1}^-1, stored at index t-1
-  for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
-    const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
-    const int t = k + 1;
-    const double* Tr = s.tmp + (size_t)t * nn + i * nx;
-    const double* Tm = s.ti + (size_t)k * nn + j;
-    double a = 0.0;
+      for (int l = 0; l < nx; ++l) a += Ti[l] * Pk[l * nx];
+      s.tmp[(size_t)t * nn + e] = a;
+    }
+    __syncthreads();
+    // P_t = -T_t theta_{t-1}^-1, stored at index t-1
+    for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
+      const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
+      const int t = k + 1;
+      const double* Tr = s.tmp + (size_t)t * nn + i * nx;
+      const double* Tm = s.ti + (size_t)k * nn + j;
+      double a = 0.0;
 #pragma unroll
-    for (int l = 0; l < nx; ++l) a += Tr[l] * Tm[l * nx];
-    s.pm[(size_t)k * nn + e] = -a;
+      for (int l = 0; l < nx; ++l) a += Tr[l] * Tm[l * nx];
+      s.pm[(size_t)k * nn + e] = -a;
+    }
   }
-  if (fp32_copy) {
-    // scaled basis of the FP32 PCG: W_t = Li_t phi_{t-1} Li_{t-1}^T (t = 1..N) in FP32 at
-    // block t-1; block N is zero
-    __syncthreads();  // the P_t pass above has finished reading tmp
+  if (fp32_copy && !sh_scaled_bad) {
+    // scaled basis: W_t = Li_t phi_{t-1} Li_{t-1}^T (t = 1..N) at block t-1, block N zero, in
+    // FP32 (w32, row stride ld) for the FP32 iterations and in FP64 (pm, row stride nx) for
+    // the FP64 residual and fallback
+    __syncthreads();
     // T_t = Li_t phi_{t-1} (t = 1..N) in tmp block t
     for (int w = threadIdx.x; w < N * nn; w += blockDim.x) {
       const int k = w / nn, e = w - k * nn, i = e / nx, j = e - i * nx;
@@ -504,16 +511,15 @@ __device__ __noinline__ void assemble_schur_t(const Inst& s, bool fp32_copy) {
     const int nl = nx * ld;
     for (int w = threadIdx.x; w < K * nl; w += blockDim.x) {
       const int k = w / nl, e = w - k * nl, i = e / ld, j = e - i * ld;
-      float v = 0.0f;
+      double v = 0.0;
       if (j < nx && k < N) {
         const double* Tr = s.tmp + (size_t)(k + 1) * nn + i * nx;
         const double* Lm = s.li + (size_t)k * nn + j * nx;  // (Li_{t-1}^T)[l][j] = Li_{t-1}[j][l]
-        double a = 0.0;
 #pragma unroll
-        for (int l = 0; l < nx; ++l) a += Tr[l] * Lm[l];
-        v = (float)a;
+        for (int l = 0; l < nx; ++l) v += Tr[l] * Lm[l];
       }
-      s.w32[w] = v;
+      s.w32[w] = (float)v;
+      if (j < nx) s.pm[(size_t)k * nn + i * nx + j] = v;
     }
   }
   __syncthreads();
@@ -678,16 +684,130 @@ __device__ __noinline__ PcgOut pcg_fp64(const Inst& s, double* lv, double* rv, d
   return PcgOut{it, eta};
 }
 
+// (L_t^-1 v_t)_i = sum_{j <= i} Li_t[i][j] v_t[j]   (FP64 vector with row stride nx)
+__device__ __forceinline__ double lower_row(const double* __restrict__ li, int nx, int t, int i,
+                                            const double* __restrict__ v) {
+  const double* m = li + ((size_t)t * nx + i) * nx;
+  const double* x = v + (size_t)t * nx;
+  double a = 0.0;
+  for (int j = 0; j <= i; ++j) a = fma(m[j], x[j], a);
+  return a;
+}
+
+// (L_t^-T v_t)_i = sum_{j >= i} Li_t[j][i] v_t[j]   (v_t: one FP32 vector segment)
+__device__ __forceinline__ double lower_col(const double* __restrict__ li, int nx, int t, int i,
+                                            const float* __restrict__ vt) {
+  const double* m = li + (size_t)t * nx * nx + i;
+  double a = 0.0;
+  for (int j = i; j < nx; ++j) a = fma(m[(size_t)j * nx], (double)vt[j], a);
+  return a;
+}
+
+// (L_t^-T v_t)_i for an FP64 vector with row stride nx
+__device__ __forceinline__ double lower_col64(const double* __restrict__ li, int nx, int t, int i,
+                                              const double* __restrict__ vt) {
+  const double* m = li + (size_t)t * nx * nx + i;
+  double a = 0.0;
+  for (int j = i; j < nx; ++j) a = fma(m[(size_t)j * nx], vt[j], a);
+  return a;
+}
+
+// (F^ v)_{t,i} in FP64 from the W blocks kept with row stride nx (block t-1 holds W_t, block
+// N is zero) for an unpadded FP64 vector v with row stride nx.
+__device__ __forceinline__ double fhat64_row(const double* __restrict__ w, int nx, int N, int t, int i,
+                                             const double* __restrict__ v) {
+  const int nn = nx * nx;
+  double a = 0.0, c = 0.0;
+  if (t > 0) {
+    const double* lo = w + (size_t)(t - 1) * nn + i * nx;
+    const double* vm = v + (size_t)(t - 1) * nx;
+    for (int j = 0; j < nx; ++j) a = fma(lo[j], vm[j], a);
+  }
+  if (t < N) {
+    const double* up = w + (size_t)t * nn + i;
+    const double* vp = v + (size_t)(t + 1) * nx;
+    for (int j = 0; j < nx; ++j) c = fma(up[(size_t)j * nx], vp[j], c);
+  }
+  return a + c;
+}
+
+// The FP64 fallback of the mixed path: the reference recurrence (pcg.py:350-436) in the
+// scaled basis, i.e. PCG on S^ = -(I + F^) with the preconditioner I - F^ for the
+// correction d^ from lam (r^ = L^-1 (gamma - S lam), lam += L^-T d^ at the end).  Its
+// iterates, eta and stopping rule are the reference's in exact arithmetic.  Vectors in
+// workspace regions free during the solve: r^ t1, p^ xn, u^ C, z^ tmp, d^ res.
+__device__ __noinline__ PcgOut pcg_fp64_scaled(const Inst& s, double* lam, int max_iter, double eps, double* red,
+                                               int& par) {
+  const int nx = s.nx, N = s.N, n = s.K * nx;
+  double *rh = s.t1, *pv = s.xn, *uv = s.C, *zv = s.tmp, *dv = s.res;
+  const double* w = s.pm;  // FP64 W blocks
+  for (int g = threadIdx.x; g < n; g += blockDim.x)
+    s.res[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lam, g);
+  __syncthreads();
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx;
+    rh[g] = lower_row(s.li, nx, t, g - t * nx, s.res);
+  }
+  __syncthreads();
+  double part = 0.0;
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx;
+    const double z = rh[g] - fhat64_row(w, nx, N, t, g - t * nx, rh);
+    pv[g] = z;
+    dv[g] = 0.0;
+    part += rh[g] * z;
+  }
+  double eta = block_sum(part, red, par);
+  int it = 0;
+  while ((fabs(eta) > eps && it <= max_iter - 1) || it < 1) {
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx;
+      const double u = -(pv[g] + fhat64_row(w, nx, N, t, g - t * nx, pv));
+      uv[g] = u;
+      part += pv[g] * u;
+    }
+    const double vden = block_sum(part, red, par);
+    const double alpha = eta / vden;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      dv[g] += alpha * pv[g];
+      rh[g] -= alpha * uv[g];
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx;
+      const double z = rh[g] - fhat64_row(w, nx, N, t, g - t * nx, rh);
+      zv[g] = z;
+      part += rh[g] * z;
+    }
+    const double etap = block_sum(part, red, par);
+    const double beta = etap / eta;
+    for (int g = threadIdx.x; g < n; g += blockDim.x) pv[g] = zv[g] + beta * pv[g];
+    eta = etap;
+    ++it;
+    __syncthreads();
+  }
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx;
+    lam[g] += lower_col64(s.li, nx, t, g - t * nx, dv + (size_t)t * nx);
+  }
+  __syncthreads();
+  return PcgOut{it, eta};
+}
+
 // FP32 refinement is not paying off: a refinement step cut eta64 by less than 1e4 (the
 // residual norm by less than 100x: kappa * eps32 is too close to 1 for the FP32 iterations
 // to reach their target in the true residual), or the FP32 iterations have used half of
-// pcg.max_iter.  Finish the solve with the FP64 recurrence on the FP64 blocks, keeping the
-// vectors in workspace regions that are free during the PCG (t1, xn, C).  The recurrence
+// pcg.max_iter.  Finish the solve with the FP64 recurrence (in the scaled basis, see
+// pcg_fp64_scaled).  The recurrence
 // gets the full pcg.max_iter budget of the reference's loop: the FP32 iterations before it
 // are cheaper and restart at every refinement, so they are not charged against it, and a
 // QP's reported iteration count can reach 1.5 max_iter.
 __device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, double eps, double* red, int& par) {
-  PcgOut o = pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, max_iter, eps, red, par);
+  // without Cholesky factors (sh_scaled_bad) the reference-basis blocks theta^-1, P exist instead
+  PcgOut o = sh_scaled_bad ? pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, max_iter, eps, red, par)
+                           : pcg_fp64_scaled(s, lam, max_iter, eps, red, par);
   return PcgOut{it + o.it, o.eta};
 }
 constexpr double kStagnation = 1e-4;
@@ -722,8 +842,9 @@ __device__ __forceinline__ T* as_shared(T* p) {
   return reinterpret_cast<T*>(g_dyn_smem + off);
 }
 
-// FP64 true residual for the thread's rows: res = gamma - S lam, returns the thread's
-// share of eta64 = res^T Phi64^-1 res (one barrier between the two passes).
+// FP64 true residual for the thread's rows, res = gamma - S lam, its scaled form
+// r^ = L^-1 res in t1, and the thread's share of eta64 = r^T (I - F^) r^ = res^T Phi^-1 res
+// (two barriers between the three passes).
 template <int NX, int kSlots>
 __device__ __forceinline__ double fp64_residual(const Inst& s, const double* lam, const int (&tt)[kSlots],
                                                 const int (&ii)[kSlots], const bool (&ok)[kSlots], int N) {
@@ -734,33 +855,18 @@ __device__ __forceinline__ double fp64_residual(const Inst& s, const double* lam
       s.res[g] = s.gam[g] + stencil64<NX>(s.th, s.ph, lam, tt[k], ii[k], N);
     }
   __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kSlots; ++k)
+    if (ok[k]) s.t1[tt[k] * NX + ii[k]] = lower_row(s.li, NX, tt[k], ii[k], s.res);
+  __syncthreads();
   double part = 0.0;
 #pragma unroll
   for (int k = 0; k < kSlots; ++k)
     if (ok[k]) {
       const int g = tt[k] * NX + ii[k];
-      part += s.res[g] * stencil64<NX>(s.ti, s.pm, s.res, tt[k], ii[k], N);
+      part += s.t1[g] * (s.t1[g] - fhat64_row(s.pm, NX, N, tt[k], ii[k], s.t1));
     }
   return part;
-}
-
-// (L_t^-1 v_t)_i = sum_{j <= i} Li_t[i][j] v_t[j]   (FP64 vector with row stride nx)
-__device__ __forceinline__ double lower_row(const double* __restrict__ li, int nx, int t, int i,
-                                            const double* __restrict__ v) {
-  const double* m = li + ((size_t)t * nx + i) * nx;
-  const double* x = v + (size_t)t * nx;
-  double a = 0.0;
-  for (int j = 0; j <= i; ++j) a = fma(m[j], x[j], a);
-  return a;
-}
-
-// (L_t^-T v_t)_i = sum_{j >= i} Li_t[j][i] v_t[j]   (v_t: one FP32 vector segment)
-__device__ __forceinline__ double lower_col(const double* __restrict__ li, int nx, int t, int i,
-                                            const float* __restrict__ vt) {
-  const double* m = li + (size_t)t * nx * nx + i;
-  double a = 0.0;
-  for (int j = i; j < nx; ++j) a = fma(m[(size_t)j * nx], (double)vt[j], a);
-  return a;
 }
 
 // (F^ v)_{t,i} = W_t[i,:] v_{t-1} + W_{t+1}[:,i] v_{t+1} for padded vectors (zero segments
@@ -798,12 +904,20 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
   const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
   double eta64 = 0.0, prev64 = 0.0;
   for (int ref = 0;; ++ref) {
+    // res = gamma - S lam, r^ = L^-1 res (t1), eta64 = r^T (I - F^) r^ = res^T Phi^-1 res
     for (int g = threadIdx.x; g < n; g += blockDim.x)
       s.res[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lam, g);
     __syncthreads();
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx;
+      s.t1[g] = lower_row(s.li, nx, t, g - t * nx, s.res);
+    }
+    __syncthreads();
     double part = 0.0;
-    for (int g = threadIdx.x; g < n; g += blockDim.x)
-      part += s.res[g] * stencil_row<double, double>(s.ti, s.pm, nx, nx, N, s.res, g);
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx;
+      part += s.t1[g] * (s.t1[g] - fhat64_row(s.pm, nx, N, t, g - t * nx, s.t1));
+    }
     eta64 = block_sum(part, red, par);
     const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
     if (!cont || !(eta64 == eta64)) break;
@@ -813,7 +927,7 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
     const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
       const int t = g / nx, i = g - t * nx, x = t * ld + i;
-      rv[x] = (float)(scale * lower_row(s.li, nx, t, i, s.res));
+      rv[x] = (float)(scale * s.t1[g]);
       dv[x] = 0.f;
     }
     __syncthreads();
@@ -957,8 +1071,8 @@ __device__ __noinline__ PcgOut pcg_pair_scaled(const Inst& s, double* lam, float
     const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
     d0 = 0.f;
     d1 = 0.f;
-    r0 = ok0 ? (float)(scale * lower_row(s.li, NX, tc, i0, s.res)) : 0.f;
-    r1 = ok1 ? (float)(scale * lower_row(s.li, NX, tc, i1, s.res)) : 0.f;
+    r0 = ok0 ? (float)(scale * s.t1[tc * NX + i0]) : 0.f;  // r^ = L^-1 res from fp64_residual
+    r1 = ok1 ? (float)(scale * s.t1[tc * NX + i1]) : 0.f;
     if (ok0) rv[seg + i0] = r0;
     if (ok1) rv[seg + i1] = r1;
     __syncthreads();
