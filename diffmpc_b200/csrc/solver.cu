@@ -47,6 +47,7 @@ struct DevGroup {
   int32_t ld32;         // row stride of FP32 blocks and padded vectors (pad_ld)
   int32_t blocks_smem;  // FP32 blocks: 0 workspace, 1 shared memory, 2 per instance (shared if they fit)
   uint64_t smem_block_budget;  // mode 2: shared-memory bytes available for one instance's blocks
+  uint32_t w64_off;      // mixed row-pair path: shared-memory byte offset of the FP64 W blocks (0: workspace)
   size_t ws_offset;     // byte offset of instance 0 in the workspace
   size_t ws_stride;     // bytes per instance
   int32_t pg_idx[DMPC_MAX_PARAM_GRADS];
@@ -139,6 +140,10 @@ struct Inst {
   float* w32;  // scaled-basis off-diagonal blocks W_t (FP32, row stride ld)
 };
 
+// the kernels' dynamic shared memory, visible to device functions: pointers rebuilt
+// from it let the compiler use shared-space loads instead of generic ones
+extern __shared__ __align__(16) unsigned char g_dyn_smem[];
+
 // g is the group's descriptor: G.g, or a view of it whose inputs/outputs point at one
 // step of a closed-loop rollout.
 __device__ inline Inst make_inst(const DevGroup& G, const dmpc_group& g, int i, void* ws, float* smem_blocks) {
@@ -190,6 +195,9 @@ __device__ inline Inst make_inst(const DevGroup& G, const dmpc_group& g, int i, 
   const bool use_smem = G.blocks_smem == 1 ||
                         (G.blocks_smem == 2 && (uint64_t)s.K * nx * s.ld * sizeof(float) <= G.smem_block_budget);
   s.w32 = use_smem ? smem_blocks : reinterpret_cast<float*>(base + L.n_doubles);
+  // the row-pair PCG reads the FP64 W blocks at every residual replacement: keep them in
+  // shared memory when the launch reserved room for them
+  if (G.w64_off) s.pm = reinterpret_cast<double*>(g_dyn_smem + G.w64_off);
   return s;
 }
 
@@ -811,6 +819,17 @@ __device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, 
   return PcgOut{it + o.it, o.eta};
 }
 constexpr double kStagnation = 1e-4;
+// Residual-replacement PCG (pcg_pair_scaled): the FP64 convergence test runs once the
+// FP32 recursion's eta is below kCheckMargin * eps, and a replacement after which the
+// FP64 eta fell by less than 1/kUpdateStagnation hands the solve to the FP64 recurrence.
+constexpr double kCheckMargin = 0.1;
+constexpr double kUpdateStagnation = 1e-2;
+// A replaced residual whose eta exceeds the recursion's previous eta by this factor
+// restarts the search direction.
+constexpr double kRestartRatio = 10.0;
+// The FP32 recursion's eta rising this far above its value at the last replacement
+// triggers a replacement (and, without true progress, the FP64 recurrence).
+constexpr double kDivergeRatio = 1e4;
 
 // ---------------------------------------------------------------- PCG, FP32 in a scaled basis + FP64 refinement
 // Scaled basis.  With the FP64 Cholesky factors theta_t = L_t L_t^T (L block diagonal)
@@ -825,16 +844,19 @@ constexpr double kStagnation = 1e-4;
 // reads only the W blocks: one off-diagonal block per stage instead of the six blocks
 // per knot of S and Phi^-1, and the unit diagonal needs no storage.
 //
-// Refinement (FP64, workspace): res = gamma - S lam and eta64 = res^T Phi^-1 res from the
-// FP64 blocks; stop like the reference on eta64 (pcg.py:397-403); otherwise run the FP32
-// PCG on S^ d^ = L^-1 res / sqrt(eta64) to a relative eta reduction of `inner_rel_tol`
-// (and to 0.01 eps in absolute terms) and update lam += sqrt(eta64) L^-T d^.  A
-// refinement that cuts eta64 by less than 100x, or the max_ref-th refinement, hands the
-// solve to the FP64 recurrence (fp64_finish).
+// FP64 correction, two forms.
+// * Any nx (pcg_mixed_scaled): iterative refinement.  res = gamma - S lam and
+//   eta64 = res^T Phi^-1 res in FP64; stop like the reference on eta64 (pcg.py:397-403);
+//   otherwise run the FP32 PCG on S^ d^ = L^-1 res / sqrt(eta64) to a relative eta
+//   reduction of `inner_rel_tol` (and to 0.01 eps in absolute terms) and update
+//   lam += sqrt(eta64) L^-T d^.  A refinement that cuts eta64 by less than 1e4, or the
+//   max_ref-th refinement, hands the solve to the FP64 recurrence (fp64_finish).
+// * Row pairs (pcg_pair_scaled): one FP32 PCG whose recursively updated residual is
+//   replaced by the FP64 residual each time its eta has fallen by `inner_rel_tol`, keeping
+//   the search direction (reliable updates: no Krylov space is thrown away at a restart).
+//   The replacement residual is formed in the scaled basis from the FP64 W blocks,
+//   r^ = r^_0 + (I + F^) lam^; the stopping test always uses an exact gamma - S lam.
 
-// the kernels' dynamic shared memory, visible to device functions: pointers rebuilt
-// from it let the compiler use shared-space loads instead of generic ones
-extern __shared__ __align__(16) unsigned char g_dyn_smem[];
 
 template <class T>
 __device__ __forceinline__ T* as_shared(T* p) {
@@ -842,31 +864,65 @@ __device__ __forceinline__ T* as_shared(T* p) {
   return reinterpret_cast<T*>(g_dyn_smem + off);
 }
 
-// FP64 true residual for the thread's rows, res = gamma - S lam, its scaled form
-// r^ = L^-1 res in t1, and the thread's share of eta64 = r^T (I - F^) r^ = res^T Phi^-1 res
-// (two barriers between the three passes).
-template <int NX, int kSlots>
-__device__ __forceinline__ double fp64_residual(const Inst& s, const double* lam, const int (&tt)[kSlots],
-                                                const int (&ii)[kSlots], const bool (&ok)[kSlots], int N) {
-#pragma unroll
-  for (int k = 0; k < kSlots; ++k)
-    if (ok[k]) {
-      const int g = tt[k] * NX + ii[k];
-      s.res[g] = s.gam[g] + stencil64<NX>(s.th, s.ph, lam, tt[k], ii[k], N);
-    }
+// Compile-time-nx FP64 helpers of the row-pair PCG (pcg_pair_scaled), rows i0, i1 of knot
+// t.  Both stay out of line, so that their registers do not weigh on the allocation of the
+// FP32 iteration loop that calls them on its cold path.
+//
+// res = gamma - S lam for the thread's rows and r^ = L^-1 res in t1 (one barrier between
+// the passes; each thread reads back only its own t1 rows).
+template <int NX>
+__device__ __noinline__ void exact_rhat(const Inst& s, const double* lam, int t, int i0, int i1, bool ok0,
+                                        bool ok1, int N) {
+  const int g0 = t * NX + i0, g1 = t * NX + i1;
+  if (ok0) s.res[g0] = s.gam[g0] + stencil64<NX>(s.th, s.ph, lam, t, i0, N);
+  if (ok1) s.res[g1] = s.gam[g1] + stencil64<NX>(s.th, s.ph, lam, t, i1, N);
   __syncthreads();
+  const double* m0 = s.li + (size_t)g0 * NX;
+  const double* m1 = s.li + (size_t)g1 * NX;
+  const double* x = s.res + t * NX;
+  double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-  for (int k = 0; k < kSlots; ++k)
-    if (ok[k]) s.t1[tt[k] * NX + ii[k]] = lower_row(s.li, NX, tt[k], ii[k], s.res);
-  __syncthreads();
-  double part = 0.0;
+  for (int j = 0; j < NX; ++j) {
+    const double xj = x[j];
+    if (j <= i0) a0 = fma(m0[j], xj, a0);
+    if (j <= i1) a1 = fma(m1[j], xj, a1);
+  }
+  if (ok0) s.t1[g0] = a0;
+  if (ok1) s.t1[g1] = a1;
+}
+
+// (F^ v) for the two rows in FP64: W_t (block t-1 of w, row stride NX) times v_{t-1} plus
+// W_{t+1}^T (block t) times v_{t+1}; block N is zero and stands in for W_0 and W_{N+1}.
+// v points at knot 0 of a vector with zero segments at knots -1 and K.
+template <int NX>
+__device__ __noinline__ double2 fhat64_pair(const double* __restrict__ w, int N, int t, int i0, int i1,
+                                            const double* v) {
+  constexpr int BS = NX * NX;
+  const double* lo = w + (size_t)(t > 0 ? t - 1 : N) * BS;
+  const double* up = w + (size_t)(t < N ? t : N) * BS;
+  const double* vm = v + (t - 1) * NX;
+  const double* vp = v + (t + 1) * NX;
+  double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
 #pragma unroll
-  for (int k = 0; k < kSlots; ++k)
-    if (ok[k]) {
-      const int g = tt[k] * NX + ii[k];
-      part += s.t1[g] * (s.t1[g] - fhat64_row(s.pm, NX, N, tt[k], ii[k], s.t1));
-    }
-  return part;
+  for (int j = 0; j < NX; ++j) {
+    const double ym = vm[j], yp = vp[j];
+    a0 = fma(lo[i0 * NX + j], ym, a0);
+    a1 = fma(lo[i1 * NX + j], ym, a1);
+    b0 = fma(up[j * NX + i0], yp, b0);
+    b1 = fma(up[j * NX + i1], yp, b1);
+  }
+  return make_double2(a0 + b0, a1 + b1);
+}
+
+// (L_t^-T v_t)_i for an FP64 vector segment v_t
+template <int NX>
+__device__ __forceinline__ double lower_col_t(const double* __restrict__ li, int t, int i, const double* vt) {
+  const double* m = li + (size_t)t * NX * NX + i;
+  double a = 0.0;
+#pragma unroll
+  for (int j = 0; j < NX; ++j)
+    if (j >= i) a = fma(m[j * NX], vt[j], a);
+  return a;
 }
 
 // (F^ v)_{t,i} = W_t[i,:] v_{t-1} + W_{t+1}[:,i] v_{t+1} for padded vectors (zero segments
@@ -996,7 +1052,7 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
 // every address in range; they take part in the barriers and reductions with zeros.
 template <int NX>
 __device__ __noinline__ PcgOut pcg_pair_scaled(const Inst& s, double* lam, float* vec, int max_iter, double eps,
-                                               int max_ref, double inner_rel, double* red, int& par) {
+                                               int max_ref, double upd_rel, double* red, int& par) {
   constexpr int LD = pad_ld(NX);
   constexpr int BS = NX * LD;
   constexpr int H = (NX + 1) / 2;
@@ -1055,43 +1111,103 @@ __device__ __noinline__ PcgOut pcg_pair_scaled(const Inst& s, double* lam, float
     f0 = a0 + b0;
     f1 = a1 + b1;
   };
-  int tt[2] = {tc, tc}, ii[2] = {i0, i1};
-  bool ok[2] = {ok0, ok1};
-  float r0 = 0.f, r1 = 0.f, p0 = 0.f, p1 = 0.f, d0 = 0.f, d1 = 0.f;
-  int it = 0;
-  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
-  double eta64 = 0.0, prev64 = 0.0;
-  for (int ref = 0;; ++ref) {
-    eta64 = block_sum2(fp64_residual<NX, 2>(s, lam, tt, ii, ok, N), red, par);
-    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
-    if (!cont || !(eta64 == eta64)) break;
-    if (ref >= max_ref || it >= it_cap || (ref > 0 && eta64 > kStagnation * prev64))
-      return fp64_finish(s, lam, it, max_iter, eps, red, par);
-    prev64 = eta64;
-    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
-    d0 = 0.f;
-    d1 = 0.f;
-    r0 = ok0 ? (float)(scale * s.t1[tc * NX + i0]) : 0.f;  // r^ = L^-1 res from fp64_residual
-    r1 = ok1 ? (float)(scale * s.t1[tc * NX + i1]) : 0.f;
-    if (ok0) rv[seg + i0] = r0;
-    if (ok1) rv[seg + i1] = r1;
+  // FP64 exchange vector (knots -1..K) in the shared vector slots the pair path leaves free,
+  // followed by the solve's constants (cst).  Everything the residual replacements need is
+  // re-derived there from s, vec and cst, so that none of it occupies registers of the
+  // iteration loop.
+  auto x64_of = [&]() { return reinterpret_cast<double*>(as_shared(vec + 2 * (K + 2) * LD)) + NX; };
+  {
+    double* x64 = x64_of();
+    for (int w = threadIdx.x; w < NX; w += blockDim.x) {
+      x64[w - NX] = 0.0;
+      x64[K * NX + w] = 0.0;
+    }
+  }
+  // r^ rows (rh) -> z^ = r^ - F^ r^ rows (zh); returns the thread's share of eta = r^.z^
+  auto eta_of = [&](double rh0, double rh1, double& zh0, double& zh1) -> double {
+    double* x64 = x64_of();
     __syncthreads();
-    float f0, f1;
-    fhat(rv, f0, f1);
-    p0 = r0 - f0;
-    p1 = r1 - f1;
-    if (ok0) pv[seg + i0] = p0;
-    if (ok1) pv[seg + i1] = p1;
-    double part = (ok0 ? (double)r0 * (double)p0 : 0.0) + (ok1 ? (double)r1 * (double)p1 : 0.0);
-    double eta = block_sum2(part, red, par);
-    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
-    int inner = 0;
-    while ((eta > target && it < it_cap) || inner < 1) {
+    if (ok0) x64[tc * NX + i0] = rh0;
+    if (ok1) x64[tc * NX + i1] = rh1;
+    __syncthreads();
+    const double2 h = fhat64_pair<NX>(s.pm, N, tc, i0, i1, x64);
+    zh0 = rh0 - h.x;
+    zh1 = rh1 - h.y;
+    return (ok0 ? rh0 * zh0 : 0.0) + (ok1 ? rh1 * zh1 : 0.0);
+  };
+  // lam += L^-T acc, acc = 0 (acc: lam^ accumulated since the last exact residual, FP64 in tmp)
+  auto flush = [&]() {
+    double* acc = s.tmp;
+    __syncthreads();
+    const double l0 = lower_col_t<NX>(s.li, tc, i0, acc + tc * NX);
+    const double l1 = lower_col_t<NX>(s.li, tc, i1, acc + tc * NX);
+    __syncthreads();
+    if (ok0) {
+      lam[tc * NX + i0] += l0;
+      acc[tc * NX + i0] = 0.0;
+    }
+    if (ok1) {
+      lam[tc * NX + i1] += l1;
+      acc[tc * NX + i1] = 0.0;
+    }
+    __syncthreads();
+  };
+  float r0, r1, p0, p1, d0 = 0.f, d1 = 0.f, f0, f1;
+  int it = 0;
+  double eta, trig, hi;
+  {
+    const int g0 = tc * NX + i0, g1 = tc * NX + i1;
+    if (ok0) s.tmp[g0] = 0.0;
+    if (ok1) s.tmp[g1] = 0.0;
+    double zh0, zh1;
+    exact_rhat<NX>(s, lam, tc, i0, i1, ok0, ok1, N);
+    const double rh0 = ok0 ? s.t1[g0] : 0.0, rh1 = ok1 ? s.t1[g1] : 0.0;
+    const double eta64 = block_sum2(eta_of(rh0, rh1, zh0, zh1), red, par);
+    if (!(eta64 == eta64)) return PcgOut{it, eta64};
+    // The FP32 vectors carry the problem scaled by 1/sqrt(eta64) of the first residual
+    // (eta starts at 1) and keep that scale through every replacement.  cst: scale,
+    // sqrt(eta64_0), scale^2, the convergence-check level, eta64 and the scaled eta at the
+    // last replacement, eps, upd_rel, max_ref, the replacement count, max_iter.
+    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+    double* cst = x64_of() + (K + 1) * NX;
+    if (threadIdx.x == 0) {
+      cst[0] = scale;
+      cst[1] = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+      cst[2] = scale * scale;
+      cst[3] = eps * scale * scale * kCheckMargin;
+      cst[4] = eta64;
+      cst[5] = eta64 * scale * scale;
+      cst[6] = eps;
+      cst[7] = upd_rel;
+      cst[8] = (double)max_ref;
+      cst[9] = 0.0;
+      cst[10] = (double)max_iter;
+    }
+    r0 = (float)(scale * rh0);
+    r1 = (float)(scale * rh1);
+    p0 = (float)(scale * zh0);
+    p1 = (float)(scale * zh1);
+    eta = eta64 * scale * scale;
+    // a replacement is due once the recursion's eta is at or below trig, above hi (the
+    // recursion diverges: FP32 cannot resolve this system) or not a number
+    trig = fmax(eps * scale * scale * kCheckMargin, upd_rel * eta);
+    hi = kDivergeRatio * eta;
+  }
+  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
+  if (ok0) pv[seg + i0] = p0;
+  if (ok1) pv[seg + i1] = p1;
+  __syncthreads();
+  double eta64 = 0.0;
+  for (;;) {
+    // FP32 iterations until a replacement is due (a tight loop of its own)
+    double vden, etap;
+    float z0, z1;
+    for (;;) {
       // u^ = S^ p^ = -(p^ + F^ p^)
       fhat(pv, f0, f1);
       const float u0 = -(p0 + f0), u1 = -(p1 + f1);
-      part = (ok0 ? (double)p0 * (double)u0 : 0.0) + (ok1 ? (double)p1 * (double)u1 : 0.0);
-      const double vden = block_sum2(part, red, par);
+      double part = (ok0 ? (double)p0 * (double)u0 : 0.0) + (ok1 ? (double)p1 * (double)u1 : 0.0);
+      vden = block_sum2(part, red, par);
       const float alpha = (float)(eta / vden);
       d0 = fmaf(alpha, p0, d0);
       d1 = fmaf(alpha, p1, d1);
@@ -1102,27 +1218,99 @@ __device__ __noinline__ PcgOut pcg_pair_scaled(const Inst& s, double* lam, float
       __syncthreads();
       // z^ = Phi^ r^ = r^ - F^ r^
       fhat(rv, f0, f1);
-      const float z0 = r0 - f0, z1 = r1 - f1;
+      z0 = r0 - f0;
+      z1 = r1 - f1;
       part = (ok0 ? (double)r0 * (double)z0 : 0.0) + (ok1 ? (double)r1 * (double)z1 : 0.0);
-      const double etap = block_sum2(part, red, par);
+      etap = block_sum2(part, red, par);
+      ++it;
+      if (!(etap > trig) || etap > hi || it >= it_cap || !(vden == vden)) break;
       const float beta = (float)(etap / eta);
       p0 = fmaf(beta, p0, z0);
       p1 = fmaf(beta, p1, z1);
       if (ok0) pv[seg + i0] = p0;
       if (ok1) pv[seg + i1] = p1;
       eta = etap;
-      ++it;
-      ++inner;
       __syncthreads();
-      if (!(eta == eta) || !(vden == vden)) break;
     }
-    // lam += sqrt(eta64) L^-T d^, with d^ published over r^ (no thread reads r^ any more)
-    if (ok0) rv[seg + i0] = d0;
-    if (ok1) rv[seg + i1] = d1;
-    __syncthreads();
-    const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
-    if (ok0) lam[tc * NX + i0] += back * lower_col(s.li, NX, tc, i0, rv + seg);
-    if (ok1) lam[tc * NX + i1] += back * lower_col(s.li, NX, tc, i1, rv + seg);
+    {
+      // Residual replacement.  acc += sqrt(eta64_0) d^ (FP64); the true scaled residual
+      // r^ = r^_0 + (I + F^) acc (r^_0 = t1, the residual at the last exact evaluation)
+      // replaces the recursively updated one and the search direction is kept.  The
+      // convergence decision always rests on an exact residual gamma - S lam.
+      double* cst = x64_of() + (K + 1) * NX;
+      double* acc = s.tmp;
+      const int g0 = tc * NX + i0, g1 = tc * NX + i1;
+      const double scale = cst[0], back = cst[1], s2 = cst[2], check_at = cst[3], prev64 = cst[4],
+                   eta_upd = cst[5], c_eps = cst[6], c_upd = cst[7];
+      const int c_maxref = (int)cst[8], nupd = (int)cst[9] + 1, c_maxit = (int)cst[10];
+      const bool bad = !(etap == etap) || !(vden == vden);
+      const bool at_check = etap <= check_at;
+      const bool progressed = etap <= c_upd * eta_upd || etap > hi;
+      // a non-finite segment is dropped: lam keeps the last finite update
+      double a0 = ok0 ? acc[g0] : 0.0, a1 = ok1 ? acc[g1] : 0.0;
+      if (!bad) {
+        a0 += back * (double)d0;
+        a1 += back * (double)d1;
+        if (ok0) acc[g0] = a0;
+        if (ok1) acc[g1] = a1;
+      }
+      d0 = 0.f;
+      d1 = 0.f;
+      double rh0, rh1, zh0, zh1;
+      bool exact = bad || at_check || it >= it_cap;
+      if (!exact) {
+        double* x64 = x64_of();
+        __syncthreads();
+        if (ok0) x64[g0] = a0;
+        if (ok1) x64[g1] = a1;
+        __syncthreads();
+        const double2 h = fhat64_pair<NX>(s.pm, N, tc, i0, i1, x64);
+        rh0 = ok0 ? s.t1[g0] + a0 + h.x : 0.0;
+        rh1 = ok1 ? s.t1[g1] + a1 + h.y : 0.0;
+        eta64 = block_sum2(eta_of(rh0, rh1, zh0, zh1), red, par);
+        exact = !(eta64 > c_eps);
+      }
+      if (exact) {
+        flush();
+        exact_rhat<NX>(s, lam, tc, i0, i1, ok0, ok1, N);
+        rh0 = ok0 ? s.t1[g0] : 0.0;
+        rh1 = ok1 ? s.t1[g1] : 0.0;
+        eta64 = block_sum2(eta_of(rh0, rh1, zh0, zh1), red, par);
+      }
+      if (!(fabs(eta64) > c_eps && it <= c_maxit - 1) || !(eta64 == eta64)) {
+        if (!exact) flush();
+        break;
+      }
+      const double etas = eta64 * s2;
+      if (bad || nupd >= c_maxref || it >= it_cap || !(etas > 0.0) ||
+          (progressed && !at_check && eta64 > kUpdateStagnation * prev64)) {
+        if (!exact) flush();
+        return fp64_finish(s, lam, it, c_maxit, c_eps, red, par);
+      }
+      if (threadIdx.x == 0) {
+        cst[4] = eta64;
+        cst[5] = etas;
+        cst[9] = (double)nupd;
+      }
+      r0 = (float)(scale * rh0);
+      r1 = (float)(scale * rh1);
+      z0 = (float)(scale * zh0);
+      z1 = (float)(scale * zh1);
+      // a true residual far above the recursion's means a stale direction: restart
+      if (etas > kRestartRatio * eta) {
+        p0 = 0.f;
+        p1 = 0.f;
+      }
+      etap = etas;
+      trig = fmax(check_at, c_upd * etas);
+      hi = kDivergeRatio * etas;
+    }
+    const float beta = (float)(etap / eta);
+    p0 = fmaf(beta, p0, z0);
+    p1 = fmaf(beta, p1, z1);
+    if (ok0) pv[seg + i0] = p0;
+    if (ok1) pv[seg + i1] = p1;
+    eta = etap;
     __syncthreads();
   }
   return PcgOut{it, eta64};
@@ -2226,9 +2414,25 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
         mode = 2;
     }
     if (p->blocks_in_smem == 1 && p->precision == DMPC_PREC_MIXED && mode != 1) return DMPC_ERR_UNSUPPORTED;
+    size_t sm = mode == 1 ? need_all : (mode == 2 ? smem_cap : base);
+    // Row-pair path (the FP32 W blocks live in registers during the iterations): the FP64
+    // W blocks of its residual replacements go to shared memory, ahead of the FP32 copy,
+    // which the pair path reads only once per QP.
+    G.w64_off = 0;
+    const int pairs = G.K * ((g.nx + 1) / 2);
+    if (p->precision == DMPC_PREC_MIXED && p->blocks_in_smem != 0 && pair_nx(g.nx) && pairs <= 512 &&
+        (p->threads_per_block == 0 || pairs <= p->threads_per_block)) {
+      const size_t w64b = (size_t)G.K * g.nx * g.nx * sizeof(double);
+      if (mode != 2 && align_up(sm, 16) + w64b <= smem_cap) {
+        G.w64_off = (uint32_t)align_up(sm, 16);
+      } else if (mode == 1 && p->blocks_in_smem != 1 && align_up(base, 16) + w64b <= smem_cap) {
+        mode = 0;
+        G.w64_off = (uint32_t)align_up(base, 16);
+      }
+      if (G.w64_off) sm = G.w64_off + w64b;
+    }
     G.blocks_smem = mode;
     G.smem_block_budget = mode == 2 ? (uint64_t)(smem_cap - base) : 0;
-    const size_t sm = mode == 1 ? need_all : (mode == 2 ? smem_cap : base);
     if (sm > smem_cap) return DMPC_ERR_UNSUPPORTED;
     if (sm > smax) smax = sm;
     int ng = 0;
@@ -2303,8 +2507,8 @@ void dmpc_default_params(dmpc_solver_params* p) {
   p->pcg_max_iter = 10000;
   p->pcg_tol_epsilon = 1e-9;
   p->precision = DMPC_PREC_MIXED;
-  p->max_refinement = 12;
-  p->inner_rel_tol = 1e-8;
+  p->max_refinement = 30;
+  p->inner_rel_tol = 1e-3;
   p->threads_per_block = 0;
   p->blocks_in_smem = -1;
 }

@@ -81,8 +81,8 @@ def solver_params_struct(params: Dict[str, Any]) -> _lib.SolverParams:
     p.pcg_tol_epsilon = float(pcg.get("tol_epsilon", 1e-9))
     prec = params.get("precision", "mixed")
     p.precision = _lib.PREC_FP64 if prec in ("fp64", _lib.PREC_FP64) else _lib.PREC_MIXED
-    p.max_refinement = int(params.get("max_refinement", 12))
-    p.inner_rel_tol = float(params.get("inner_rel_tol", 1e-8))
+    p.max_refinement = int(params.get("max_refinement", 30))
+    p.inner_rel_tol = float(params.get("inner_rel_tol", 1e-3))
     p.threads_per_block = int(params.get("threads_per_block", 0))
     p.blocks_in_smem = int(params.get("blocks_in_smem", -1))
     return p

@@ -98,8 +98,10 @@ typedef struct dmpc_solver_params {
                                      an FP64 fallback recurrence then gets a full budget of its own */
   double pcg_tol_epsilon;         /* sqp.yaml pcg.tol_epsilon (absolute, on eta = r^T Phi^-1 r) */
   int32_t precision;              /* DMPC_PREC_* */
-  int32_t max_refinement;         /* MIXED: outer FP64 refinement steps per QP solve */
-  double inner_rel_tol;           /* MIXED: inner FP32 PCG stops when eta32 <= inner_rel_tol * eta at restart */
+  int32_t max_refinement;         /* MIXED: FP64 residual evaluations per QP solve (replacements in the
+                                     row-pair PCG, restarts otherwise) before the FP64 fallback */
+  double inner_rel_tol;           /* MIXED: the FP32 recursion's eta falls by this factor between FP64
+                                     residual replacements (row-pair PCG) or restarts (other nx) */
   int32_t threads_per_block;      /* 0 = automatic: one thread per row pair of the FP32 PCG (else per row),
                                      256..512; or 64..512, a multiple of 32 (diffmpc_b200.autotune) */
   int32_t blocks_in_smem;         /* MIXED, the FP32 scaled off-diagonal blocks: -1 shared memory when they
