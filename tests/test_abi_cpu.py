@@ -40,6 +40,22 @@ def test_defaults_match_reference_yaml():
     assert p.warm_start_backward == 1 and p.pcg_max_iter == 10000 and p.pcg_tol_epsilon == 1e-9
 
 
+def test_mixed_precision_defaults_agree_everywhere():
+    """The C defaults, the Python fallbacks and the package's sqp.yaml give the same mixed-path
+    knobs, so a solver built from the YAML runs the tuned configuration."""
+    from diffmpc_b200.problem import load_solver_params
+    from diffmpc_b200.sqp import solver_params_struct
+
+    c = _lib.SolverParams()
+    _lib.load().dmpc_default_params(c)
+    from_yaml = solver_params_struct(load_solver_params("sqp.yaml"))
+    from_empty = solver_params_struct({})
+    for q in (from_yaml, from_empty):
+        assert q.inner_rel_tol == c.inner_rel_tol == 1e-3
+        assert q.max_refinement == c.max_refinement == 30
+        assert q.precision == c.precision == _lib.PREC_MIXED
+
+
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc missing")
 def test_struct_layout_matches_c(tmp_path):
     src = tmp_path / "layout.c"
