@@ -347,7 +347,7 @@ def run_ours(args):
         e1.record()
         torch.cuda.synchronize()
         fp64_rate = S / (e0.elapsed_time(e1) * 1e-3)
-        ctrl64 = torch.cat([s.controls for s in sols64]).cpu()
+        ctrl64 = torch.cat([s.controls.detach() for s in sols64]).cpu()
         rel64 = float((sol.controls[:S].detach().cpu() - ctrl64).abs().max() / ctrl64.abs().max())
         line["fp64_one_per_launch"] = {
             "value": fp64_rate, "unit": UNIT, "sample": f"{S} instances, one fwd+adj launch pair each",

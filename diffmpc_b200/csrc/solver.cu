@@ -1539,6 +1539,16 @@ __device__ __forceinline__ void sqp_forward(const DevGroup& G, const dmpc_group&
   if (threadIdx.x == 0) sh_inst = make_inst(G, g, ii, ws, sv.blocks);
   __syncthreads();
   const Inst& s = sh_inst;
+  if (s.N < 1 || s.N > g.horizon) {
+    // per-instance horizon outside [1, horizon]: reported, not solved (the host does not read
+    // the horizons back, so the check lives here)
+    if (threadIdx.x == 0) {
+      g.status[ii] = DMPC_STATUS_ERROR;
+      g.num_iter[ii] = 0;
+      g.convergence_error[ii] = __longlong_as_double(0x7ff8000000000000ll);
+    }
+    return;
+  }
   const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K;
   const int maxit = P.num_scp_iteration_max;
   double* gx = g.states + (size_t)ii * Kmax * nx;
@@ -1794,6 +1804,7 @@ __device__ __forceinline__ void sqp_adjoint(const DevGroup& G, const dmpc_group&
   if (threadIdx.x == 0) sh_inst = make_inst(G, g, ii, ws, sv.blocks);
   __syncthreads();
   const Inst& s = sh_inst;
+  if (s.N < 1 || s.N > g.horizon) return;  // invalid horizon: the forward marked it ERROR
   const int nx = s.nx, nu = s.nu, Kmax = G.K, K = s.K, N = s.N;
   const size_t ox = (size_t)ii * Kmax * nx, ou = (size_t)ii * Kmax * nu;
   int par = 0;

@@ -3,9 +3,10 @@
 ``make_jax_solve(solver)`` returns ``solve(x0, weights) -> (states, controls)``.
 - It is differentiable with ``jax.grad`` w.r.t. ``weights``, a dict of float64 arrays.
 - Its forward and backward run the CUDA kernels through ``jax.pure_callback``, handing the arrays over via host memory. This keeps existing JAX code (``jit``, ``grad``) working unchanged.
-- A zero-copy binding registers the C entry points as XLA FFI custom calls instead.
+- A zero-copy binding registers the C entry points as XLA FFI custom calls instead; the
+  handler that maps XLA buffers onto the C ABI is ``csrc/xla_ffi.cc``.
 
-JAX and jaxlib cannot be installed in this build's offline image, so this module is
+JAX and jaxlib are not installed in the image this library is built in, so this module is
 import-guarded and untested there.  ``make_jax_solve`` raises ImportError without jax.
 """
 

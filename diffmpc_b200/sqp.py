@@ -126,9 +126,12 @@ class _Call:
         hz = params.get("horizons", None)
         self.horizons = None
         if hz is not None:
-            self.horizons = torch.as_tensor(hz, dtype=torch.int32, device=device).reshape(B).contiguous()
-            if int(self.horizons.min()) < 1 or int(self.horizons.max()) > N:
+            t = torch.as_tensor(hz)
+            if t.device.type == "cpu" and t.numel() > 0 and (int(t.min()) < 1 or int(t.max()) > N):
                 raise ValueError("per-instance horizons must lie in [1, horizon]")
+            # a device tensor is not read back (no host sync): the kernels mark an instance
+            # whose horizon lies outside [1, horizon] with status ERROR and leave it unsolved
+            self.horizons = t.to(device=device, dtype=torch.int32).reshape(B).contiguous()
         # guess -> outputs (the kernel works in place)
         self.states = f(guess.states, K, nx).clone()
         self.controls = f(guess.controls, K, nu).clone()
