@@ -11,6 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdmpc.so")
 
+ABI_VERSION = 2
 DMPC_OK = 0
 DMPC_ERR_CUDA = 3
 DMPC_MAX_NX = 32
@@ -22,6 +23,7 @@ DMPC_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 MODEL_IDS = {"linear": 0, "quadrotor": 1, "spacecraft": 2, "attitude": 3, "cartpole": 4}
 PREC_FP64, PREC_MIXED = 0, 1
+CTA_AUTO, CTA_WIDE, CTA_ROWS, CTA_DUAL = 0, 1, 2, 3
 SIM_LINEAR, SIM_MODEL, SIM_MODEL_SCHEME = 0, 1, 2
 
 EXPORTED_SYMBOLS = (
@@ -65,6 +67,7 @@ class SolverParams(ctypes.Structure):
         ("inner_rel_tol", _f64),
         ("threads_per_block", _i32),
         ("blocks_in_smem", _i32),
+        ("cta_config", _i32),
     ]
 
 
@@ -226,7 +229,7 @@ def load():
         ctypes.POINTER(Group), ctypes.POINTER(Rollout), ctypes.POINTER(Adjoint), ctypes.POINTER(RolloutAdjoint),
         ctypes.POINTER(SolverParams), _p, ctypes.c_size_t, _p,
     ]
-    if lib.dmpc_abi_version() != 1:
+    if lib.dmpc_abi_version() != ABI_VERSION:
         raise DmpcError("libdmpc.so ABI version mismatch")
     _lib = lib
     return lib

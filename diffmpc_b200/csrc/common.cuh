@@ -31,6 +31,42 @@ __device__ __forceinline__ double block_sum(double v, double* red, int& parity) 
   return s;
 }
 
+// CTA-wide sum of per-thread FP32 partials: an FP32 butterfly inside each warp, then an FP64
+// butterfly of width w2 (a power of two >= the warp count) over the warp sums.  Every thread
+// gets the same value: a butterfly adds the same two operands in every lane of a pair, and
+// addition is commutative.  `red` holds 2 x 64 doubles used alternately, as in block_sum.
+__device__ __forceinline__ double block_sum_f32w(float v, double* red, int& parity, int w2) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(DMPC_FULL_MASK, v, o);
+  double* buf = red + (parity << 6);
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) buf[threadIdx.x >> 5] = (double)v;
+  __syncthreads();
+  const int l = lane & (w2 - 1);
+  double s = (l < (int)(blockDim.x >> 5)) ? buf[l] : 0.0;
+  for (int o = w2 >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(DMPC_FULL_MASK, s, o);
+  parity ^= 1;
+  return s;
+}
+
+// Smallest power of two >= the CTA's warp count (the width of block_sum_f32w's second stage).
+__device__ __forceinline__ int warp_pow2() {
+  const int nw = blockDim.x >> 5;
+  int w = 1;
+  while (w < nw) w <<= 1;
+  return w;
+}
+
+// a / b rounded to FP32, for the FP32 step lengths of the PCG recursion: an FP32 division of the
+// rounded operands while both are normal floats away from the ends of the range (one FP32
+// rounding more than (float)(a / b)), else the FP64 quotient rounded.  NaN takes the FP64 path.
+__device__ __forceinline__ float quot32(double a, double b) {
+  const float fa = (float)a, fb = (float)b;
+  const float aa = fabsf(fa), ab = fabsf(fb);
+  if (aa >= 1e-30f && ab >= 1e-30f && aa <= 1e30f && ab <= 1e30f) return fa / fb;
+  return (float)(a / b);
+}
+
 // CTA-wide max.  NaN propagates (a NaN operand makes the result NaN).
 __device__ __forceinline__ double block_max(double v, double* red, int& parity) {
   bool nan = v != v;

@@ -85,6 +85,7 @@ def solver_params_struct(params: Dict[str, Any]) -> _lib.SolverParams:
     p.inner_rel_tol = float(params.get("inner_rel_tol", 1e-3))
     p.threads_per_block = int(params.get("threads_per_block", 0))
     p.blocks_in_smem = int(params.get("blocks_in_smem", -1))
+    p.cta_config = int(params.get("cta_config", 0))
     return p
 
 

@@ -32,6 +32,14 @@
  * batch).  N is the reference's `horizon`; K = N + 1 knots.  All calls are
  * stream-ordered, never synchronise the host, and never allocate: scratch
  * memory is the caller's `workspace` (size from dmpc_workspace_size).
+ *
+ * Launches are persistent: a grid of the CTAs that can be resident at once takes the
+ * instances from a work counter kept in the first 256 bytes of the workspace (zeroed by a
+ * stream-ordered memset before each launch), and each CTA solves its instances one after
+ * another in its own slot of the rest of the workspace.  The workspace therefore grows with
+ * the number of resident CTAs, not with the batch; a workspace smaller than
+ * dmpc_workspace_size but holding the counter and at least one slot also works, with fewer
+ * CTAs.  Calls that share a workspace must not overlap on the GPU.
  * Return value: DMPC_OK or a DMPC_ERR_* code; per-instance solver status is
  * written to device memory with the reference's values (0 success, -100 error).
  */
@@ -45,7 +53,7 @@
 extern "C" {
 #endif
 
-#define DMPC_ABI_VERSION 1
+#define DMPC_ABI_VERSION 2
 
 /* return codes */
 #define DMPC_OK 0
@@ -106,7 +114,17 @@ typedef struct dmpc_solver_params {
                                      256..512; or 64..512, a multiple of 32 (diffmpc_b200.autotune) */
   int32_t blocks_in_smem;         /* MIXED, the FP32 scaled off-diagonal blocks: -1 shared memory when they
                                      fit (per instance in a ragged group), 0 workspace, 1 require shared */
+  int32_t cta_config;             /* DMPC_CTA_*: CTA shape of the solver kernels (diffmpc_b200.autotune) */
 } dmpc_solver_params;
+
+/* dmpc_solver_params.cta_config.  AUTO: ROWS when every group is mixed precision with a
+ * compile-time row PCG (nx in {3,4,6,7,8,12,13}) whose K ceil(nx/4) threads fit 384 (or is ragged:
+ * its longer instances take the generic PCG), else WIDE. */
+#define DMPC_CTA_AUTO 0
+#define DMPC_CTA_WIDE 1 /* up to 512 threads (threads_per_block or automatic), one CTA per SM */
+#define DMPC_CTA_ROWS 2 /* 256..384 threads (threads_per_block or automatic), one CTA per SM, up to 168
+                           registers per thread for the row PCG */
+#define DMPC_CTA_DUAL 3 /* 256 threads, two CTAs per SM */
 
 /* One group = instances sharing model, nx, nu and max horizon (a batch).
  * Per-instance horizons may differ (ragged batch): arrays are padded to K = horizon + 1
@@ -224,7 +242,8 @@ const char* dmpc_error_string(int code);
  * surfaces XLA runtime errors as Python exceptions. */
 const char* dmpc_last_cuda_error(void);
 
-/* Bytes of workspace the forward/adjoint calls need for these groups. */
+/* Bytes of workspace the forward/adjoint calls need for these groups: the work counter plus one
+ * slot (the largest instance's scratch) per CTA that can be resident on the current device. */
 size_t dmpc_workspace_size(int n_groups, const dmpc_group* groups, const dmpc_solver_params* params);
 
 /* Fills `params` with the reference defaults (sqp.yaml:1-11) and MIXED precision. */
@@ -245,7 +264,9 @@ int dmpc_solve_fwd(int n_groups, const dmpc_group* groups, const dmpc_solver_par
  * that loads the library until the process exits.  Problems that need more scratch
  * than that (dmpc_workspace_size) are rejected with DMPC_ERR_WORKSPACE and nothing is
  * launched.  The first call on a device looks up the array's device address with that
- * device current; make that call before any stream capture.  All calls share the one
+ * device current; make that call before any stream capture.  The address is cached per device
+ * for the life of the process: after cudaDeviceReset the cached address is stale, so a process
+ * that resets a device must not call this entry point on that device again.  All calls share the one
  * array and it keeps the previous call's contents (the solver initialises everything it
  * reads), so calls that may overlap on the GPU -- on different streams, or from several
  * host threads -- race and must be serialised by the caller. */

@@ -28,7 +28,7 @@ def test_library_loads_and_exports_every_header_symbol():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(_lib.EXPORTED_SYMBOLS)
-    assert lib.dmpc_abi_version() == 1
+    assert lib.dmpc_abi_version() == _lib.ABI_VERSION == 2
 
 
 def test_defaults_match_reference_yaml():
@@ -124,14 +124,20 @@ def test_calls_return_a_named_cuda_error_without_a_device():
         _lib.check(3, "dmpc_solve_fwd")
 
 
-def test_workspace_grows_with_batch_and_horizon():
+def test_workspace_grows_with_resident_ctas_not_with_batch():
+    """The workspace is a 256-byte work counter plus one slot per CTA that can be resident: it
+    grows with the batch up to that count and then stays put (persistent launch)."""
     lib = _lib.load()
     p = _lib.SolverParams()
     lib.dmpc_default_params(p)
     a = lib.dmpc_workspace_size(1, _group(batch=1), p)
     b = lib.dmpc_workspace_size(1, _group(batch=4), p)
     c = lib.dmpc_workspace_size(1, _group(batch=1, N=20), p)
-    assert b == 4 * a and c > a and a % 256 == 0
+    big = lib.dmpc_workspace_size(1, _group(batch=100000), p)
+    huge = lib.dmpc_workspace_size(1, _group(batch=1000000), p)
+    slot = a - 256
+    assert b - 256 == 4 * slot and c > a and slot % 256 == 0
+    assert big == huge and (big - 256) % slot == 0 and (big - 256) // slot <= 4 * 1024
 
 
 def test_jax_shim_is_import_guarded():
