@@ -5,8 +5,9 @@ source under ``csrc/`` or ``include/`` is newer than the library.
 
 The SQP kernels (``csrc/k_sqp.cu``) are compiled once per launch
 configuration (``-DDMPC_CFG=0``: up to 512 threads and one CTA per SM;
-``1``: up to 384 threads, one CTA per SM, up to 168 registers a thread; ``2``:
-256 threads and two CTAs per SM), in parallel with the host side and the
+``1``: up to 256 threads, one CTA per SM, up to 255 registers a thread; ``2``:
+256 threads and two CTAs per SM; ``3``: up to 384 threads, one CTA per SM, up to
+168 registers a thread), in parallel with the host side and the
 dense-layout kernels (``csrc/solver.cu``) and the XLA custom-call handler
 core (``csrc/xla_ffi.cc``); the objects are linked into one shared library.
 """
@@ -27,6 +28,7 @@ UNITS = [
     ("k_sqp_cfg0.o", os.path.join(CSRC, "k_sqp.cu"), ["-DDMPC_CFG=0"]),
     ("k_sqp_cfg1.o", os.path.join(CSRC, "k_sqp.cu"), ["-DDMPC_CFG=1"]),
     ("k_sqp_cfg2.o", os.path.join(CSRC, "k_sqp.cu"), ["-DDMPC_CFG=2"]),
+    ("k_sqp_cfg3.o", os.path.join(CSRC, "k_sqp.cu"), ["-DDMPC_CFG=3"]),
 ]
 if os.path.exists(os.path.join(CSRC, "xla_ffi.cc")):
     UNITS.append(("xla_ffi.o", os.path.join(CSRC, "xla_ffi.cc"), []))

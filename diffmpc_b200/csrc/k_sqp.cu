@@ -1,9 +1,10 @@
 // The SQP kernels of one launch configuration and their host launch wrappers.  Compiled once
-// per configuration: -DDMPC_CFG=0 (up to 512 threads, one CTA per SM), 1 (up to 384 threads,
-// one CTA per SM with up to 168 registers a thread) and 2 (256 threads, two CTAs per SM);
-// solver.cu picks the configuration per launch.
+// per configuration: -DDMPC_CFG=0 (up to 512 threads, one CTA per SM), 1 (up to 256 threads,
+// one CTA per SM, up to 255 registers a thread), 2 (256 threads, two CTAs per SM) and 3 (up to
+// 384 threads, one CTA per SM, up to 168 registers a thread); solver.cu picks the configuration
+// per launch.
 #ifndef DMPC_CFG
-#error "compile with -DDMPC_CFG=0, 1 or 2"
+#error "compile with -DDMPC_CFG=0, 1, 2 or 3"
 #endif
 #include "sqp_device.cuh"
 

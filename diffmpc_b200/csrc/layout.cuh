@@ -12,13 +12,14 @@ namespace dmpc_impl {
 constexpr int kMaxGroups = 8;
 
 // Launch configurations of the SQP kernels (dmpc_solver_params.cta_config).  kCfgWide: up to 512
-// threads, one CTA per SM, 128 registers per thread.  kCfgRows: 256 to 384 threads, one CTA per
-// SM, up to 168 registers per thread, which the compile-time row PCG needs to keep its W
-// coefficients in registers without spilling.  kCfgDual: 256 threads, two CTAs per SM, 128
-// registers.
+// threads, one CTA per SM, 128 registers per thread.  kCfgRows: up to 256 threads, one CTA per
+// SM, up to 255 registers per thread, which the compile-time row PCG needs to keep its W
+// coefficients in registers without spilling; kCfgRows384 the same up to 384 threads (168
+// registers).  kCfgDual: 256 threads, two CTAs per SM, 128 registers.
 constexpr int kCfgWide = 0;
 constexpr int kCfgRows = 1;
 constexpr int kCfgDual = 2;
+constexpr int kCfgRows384 = 3;
 
 // Bytes at the start of every workspace that hold the persistent kernels' work counter.
 constexpr size_t kQueueBytes = 256;
@@ -144,9 +145,12 @@ cudaError_t sqp_launch_cfg1(int kind, const DevArgs& args, const LaunchExtra& ex
                             size_t smem, cudaStream_t st);
 cudaError_t sqp_launch_cfg2(int kind, const DevArgs& args, const LaunchExtra& ex, void* ws, int threads,
                             size_t smem, cudaStream_t st);
+cudaError_t sqp_launch_cfg3(int kind, const DevArgs& args, const LaunchExtra& ex, void* ws, int threads,
+                            size_t smem, cudaStream_t st);
 // resident CTAs per SM of the solver kernels (the smallest over the forward, adjoint and rollout kernels)
 int sqp_blocks_per_sm_cfg0(int threads, size_t smem);
 int sqp_blocks_per_sm_cfg1(int threads, size_t smem);
 int sqp_blocks_per_sm_cfg2(int threads, size_t smem);
+int sqp_blocks_per_sm_cfg3(int threads, size_t smem);
 
 }  // namespace dmpc_impl

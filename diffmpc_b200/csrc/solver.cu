@@ -458,6 +458,7 @@ size_t group_smem(const dmpc_solver_params* p, const dmpc_group& g, DevGroup& G,
 
 int blocks_per_sm(int cfg, int threads, size_t smem) {
   if (cfg == kCfgRows) return sqp_blocks_per_sm_cfg1(threads, smem);
+  if (cfg == kCfgRows384) return sqp_blocks_per_sm_cfg3(threads, smem);
   if (cfg == kCfgDual) return sqp_blocks_per_sm_cfg2(threads, smem);
   return sqp_blocks_per_sm_cfg0(threads, smem);
 }
@@ -533,6 +534,9 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     }
     if (thr > max_thr) thr = max_thr;
   }
+  // more than 256 threads take the 384-thread bound (168 registers a thread)
+  if (cfg == kCfgRows && thr > 256) cfg = kCfgRows384;
+  args->cfg = cfg;
   const size_t cap = cfg == kCfgDual ? cap_dual : cap_wide;
   size_t smax = 0, stride = 0;
   for (int k = 0; k < n_groups; ++k) {
@@ -588,6 +592,7 @@ int launch(int kind, DevArgs* args, const LaunchExtra& ex, void* workspace, size
   cudaError_t e = cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess) return cuda_rc(e);
   if (args->cfg == kCfgRows) e = sqp_launch_cfg1(kind, *args, ex, workspace, threads, smem, st);
+  else if (args->cfg == kCfgRows384) e = sqp_launch_cfg3(kind, *args, ex, workspace, threads, smem, st);
   else if (args->cfg == kCfgDual) e = sqp_launch_cfg2(kind, *args, ex, workspace, threads, smem, st);
   else e = sqp_launch_cfg0(kind, *args, ex, workspace, threads, smem, st);
   return cuda_rc(e);

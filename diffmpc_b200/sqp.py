@@ -19,7 +19,8 @@ from typing import Any, Dict, NamedTuple
 import torch
 
 from . import _lib
-from .pcg import PCGOptimalControl
+from .pcg import (PCGOptimalControl, QPCostParameters, QPDynamicsCostPremultipliedMatrices,
+                  QPDynamicsParameters, QPParameters)
 from .problem import OptimalControlProblem, load_solver_params
 
 DEFAULT_SOLVER_PARAMS = load_solver_params("sqp.yaml")
@@ -453,11 +454,42 @@ class SQPSolver:
         holder = {}
         states, controls, dual, dbg_out = _SQPFunction.apply(self, g, problem_params, keys, holder, dbg, *vals)
         c = holder["call"]
+        qp = premult = schur = None
+        if self._params.get("return_qp_matrices", False) and c.horizons is None:
+            qp, premult, schur = self.qp_matrices(c)
         sol = SQPSolution(
-            states, controls, dual, None, None, None,
+            states, controls, dual, qp, premult, schur,
             c.status, c.num_iter, c.conv, c.conv_hist, c.alpha_hist, c.pcg_hist, dbg_out,
             c.lin_states, c.lin_controls,
         )
         if unbatched:
-            sol = SQPSolution(*[None if v is None else (v[0] if isinstance(v, torch.Tensor) and v.dim() > 0 else v) for v in sol])
+            first = lambda v: v[0] if isinstance(v, torch.Tensor) and v.dim() > 0 else v  # noqa: E731
+            sol = SQPSolution(*[
+                None if v is None else (type(v)(*[type(w)(*[first(x) for x in w]) if isinstance(w, tuple) else first(w)
+                                                  for w in v]) if isinstance(v, tuple) else first(v))
+                for v in sol])
         return sol
+
+    def qp_matrices(self, call):
+        """QP data of the last SQP iteration, as the reference keeps it in SQPSolution
+        (qp_parameters, dynamics_cost_premultiplied_matrices, schur_complement_matrices;
+        sqp.py:44-46, set by each iteration of _solve, :436-560): the linearization at the
+        iterate the last QP was built at (dmpc_linearize), A_next = -I, the premultiplied
+        products (sqp.py:247-254) and S, Phi^-1 (dmpc_schur_assemble).  Uniform horizons only."""
+        lib = _lib.load()
+        B, K, nx, nu, N = call.B, call.K, call.nx, call.nu, call.N
+        dev = call.states.device
+        g = _lib.Group.from_buffer_copy(call.group)
+        g.states, g.controls = call.lin_states.data_ptr(), call.lin_controls.data_ptr()
+        e = lambda *sh: torch.empty(*sh, dtype=torch.float64, device=dev)  # noqa: E731
+        As, Bs, Cs, Qinv, qvec = e(B, N, nx, nx), e(B, N, nx, nu), e(B, K, nx), e(B, K, nx, nx), e(B, K, nx)
+        Rinv, rvec = e(B, N, nu, nu), e(B, N, nu)
+        n = lib.dmpc_workspace_size(1, g, self._c_params)
+        ws = self._workspace(n, dev)
+        _lib.check(lib.dmpc_linearize(g, self._c_params, As.data_ptr(), Bs.data_ptr(), Cs.data_ptr(), Qinv.data_ptr(),
+                                      qvec.data_ptr(), Rinv.data_ptr(), rvec.data_ptr(), ws.data_ptr(), ws.numel(),
+                                      torch.cuda.current_stream(dev).cuda_stream), "dmpc_linearize")
+        As_next = -torch.eye(nx, dtype=torch.float64, device=dev).expand(B, N, nx, nx).contiguous()
+        qp = QPParameters(QPDynamicsParameters(As_next, As, Bs, Cs), QPCostParameters(Qinv, qvec, Rinv, rvec))
+        premult = QPDynamicsCostPremultipliedMatrices(As @ Qinv[:, :-1], As_next @ Qinv[:, 1:], Bs @ Rinv)
+        return qp, premult, self._pcg.compute_S_Phiinv(qp)

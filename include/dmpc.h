@@ -122,8 +122,8 @@ typedef struct dmpc_solver_params {
  * its longer instances take the generic PCG), else WIDE. */
 #define DMPC_CTA_AUTO 0
 #define DMPC_CTA_WIDE 1 /* up to 512 threads (threads_per_block or automatic), one CTA per SM */
-#define DMPC_CTA_ROWS 2 /* 256..384 threads (threads_per_block or automatic), one CTA per SM, up to 168
-                           registers per thread for the row PCG */
+#define DMPC_CTA_ROWS 2 /* 256..384 threads (threads_per_block or automatic), one CTA per SM; up to 255
+                           registers per thread at 256 threads, 168 above, for the row PCG */
 #define DMPC_CTA_DUAL 3 /* 256 threads, two CTAs per SM */
 
 /* One group = instances sharing model, nx, nu and max horizon (a batch).

@@ -169,3 +169,42 @@ def test_warm_start_resolve_is_stable():
     sol2 = solver.solve(sol, workloads.to_device(bt, DEV))
     assert rel_err(sol2.controls, sol.controls) < 1e-7
     assert int(sol2.num_iter.max()) <= int(sol.num_iter.max())
+
+
+@pytest.mark.parametrize("case", ["quadrotor_rk4", "linear_lti"])
+def test_solution_qp_matrices_match_oracle(case):
+    """With return_qp_matrices the solution carries the last SQP iteration's QP data, as the
+    reference's SQPSolution does (sqp.py:44-46): dmpc_linearize (A, B, C, Q^-1, q, R^-1, r at the
+    saved linearization point), the premultiplied products and S, Phi^-1 (dmpc_schur_assemble).
+    They match the oracle's compute_qp_parameters at the same point to FP64 rounding."""
+    from tests.oracle_util import oracle_solver, tensor_params
+
+    dyn, st, bt, sp = CASES[case]()
+    sp["return_qp_matrices"] = True
+    solver, sol = gpu_solve(dyn, st, bt, sp)
+    assert sol.qp_parameters is not None and sol.schur_complement_matrices is not None
+    os_ = oracle_solver(dyn, st, sp)
+    x, u = sol.linearization_states.cpu(), sol.linearization_controls.cpu()
+    qp, premult, schur = os_.compute_qp_parameters(x, u, tensor_params(bt))
+    pairs = [
+        (sol.qp_parameters.dynamics.As, qp.dynamics.As), (sol.qp_parameters.dynamics.Bs, qp.dynamics.Bs),
+        (sol.qp_parameters.dynamics.Cs, qp.dynamics.Cs), (sol.qp_parameters.dynamics.As_next, qp.dynamics.As_next),
+        (sol.qp_parameters.cost.Qinv, qp.cost.Qinv), (sol.qp_parameters.cost.qvec, qp.cost.qvec),
+        (sol.qp_parameters.cost.Rinv, qp.cost.Rinv), (sol.qp_parameters.cost.rvec, qp.cost.rvec),
+        (sol.dynamics_cost_premultiplied_matrices.As_x_Qinv, premult.As_x_Qinv),
+        (sol.dynamics_cost_premultiplied_matrices.Asnext_x_Qinvnext, premult.Asnext_x_Qinvnext),
+        (sol.dynamics_cost_premultiplied_matrices.Bs_x_Rinv, premult.Bs_x_Rinv),
+        (sol.schur_complement_matrices.S, schur.S),
+        (sol.schur_complement_matrices.preconditioner_Phiinv, schur.preconditioner_Phiinv),
+    ]
+    for i, (a, b) in enumerate(pairs):
+        assert a.shape == b.shape, i
+        # q = J - x^T H cancels to exact zeros in the oracle where the reference trajectory is
+        # zero; relative to max(|b|, 1) the FP64 rounding left there is measured like elsewhere
+        b = b.to(torch.float64)
+        err = float((a.cpu() - b).abs().max() / max(float(b.abs().max()), 1.0))
+        assert err < 1e-10, (i, err)
+    # without the option the fields stay empty (no extra kernels on the solve path)
+    sp["return_qp_matrices"] = False
+    _, sol2 = gpu_solve(dyn, st, bt, sp)
+    assert sol2.qp_parameters is None and sol2.schur_complement_matrices is None
