@@ -700,8 +700,7 @@ __device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, 
                            : pcg_fp64_scaled(s, lam, max_iter, eps, red, par);
   return PcgOut{it + o.it, o.eta};
 }
-constexpr double kStagnation = 1e-4;
-// Residual-replacement PCG (pcg_rows_scaled): the FP64 convergence test runs once the
+// Residual-replacement PCGs (pcg_rows_scaled, pcg_mixed_scaled): the FP64 convergence test runs once the
 // FP32 recursion's eta is below kCheckMargin * eps, and a replacement after which the
 // FP64 eta fell by less than 1/kUpdateStagnation hands the solve to the FP64 recurrence.
 constexpr double kCheckMargin = 0.1;
@@ -712,6 +711,16 @@ constexpr double kRestartRatio = 10.0;
 // The FP32 recursion's eta rising this far above its value at the last replacement
 // triggers a replacement (and, without true progress, the FP64 recurrence).
 constexpr double kDivergeRatio = 1e4;
+// Stall detection: an FP32 segment (the iterations between two replacements) that runs past
+// max(kStallGrowth x the previous segment, kStallMin) iterations (kStallMin for the first) is cut
+// by a replacement, to which the stagnation rule then applies: an FP32 recursion that has
+// stopped falling on an ill-conditioned system goes to the FP64 recurrence after a few hundred
+// iterations instead of half the budget.
+constexpr int kStallMin = 200;
+constexpr int kStallGrowth = 4;
+__device__ __forceinline__ int next_stop(int it, int seg, int it_cap) {
+  return min(it_cap, it + max(kStallGrowth * seg, kStallMin));
+}
 
 // ---------------------------------------------------------------- PCG, FP32 in a scaled basis + FP64 refinement
 // Scaled basis.  With the FP64 Cholesky factors theta_t = L_t L_t^T (L block diagonal)
@@ -726,18 +735,12 @@ constexpr double kDivergeRatio = 1e4;
 // reads only the W blocks: one off-diagonal block per stage instead of the six blocks
 // per knot of S and Phi^-1, and the unit diagonal needs no storage.
 //
-// FP64 correction, two forms.
-// * Any nx (pcg_mixed_scaled): iterative refinement.  res = gamma - S lam and
-//   eta64 = res^T Phi^-1 res in FP64; stop like the reference on eta64 (pcg.py:397-403);
-//   otherwise run the FP32 PCG on S^ d^ = L^-1 res / sqrt(eta64) to a relative eta
-//   reduction of `inner_rel_tol` (and to 0.01 eps in absolute terms) and update
-//   lam += sqrt(eta64) L^-T d^.  A refinement that cuts eta64 by less than 1e4, or the
-//   max_ref-th refinement, hands the solve to the FP64 recurrence (fp64_finish).
-// * Compile-time nx (pcg_rows_scaled): one FP32 PCG whose recursively updated residual is
-//   replaced by the FP64 residual each time its eta has fallen by `inner_rel_tol`, keeping
-//   the search direction (reliable updates: no Krylov space is thrown away at a restart).
-//   The replacement residual is formed in the scaled basis from the FP64 W blocks,
-//   r^ = r^_0 + (I + F^) lam^; the stopping test always uses an exact gamma - S lam.
+// FP64 correction: residual replacement in both FP32 PCGs (pcg_rows_scaled for the nx with a
+// compile-time row layout, pcg_mixed_scaled for any nx): one FP32 PCG whose recursively updated
+// residual is replaced by the FP64 residual each time its eta has fallen by `inner_rel_tol`,
+// keeping the search direction (reliable updates: no Krylov space is thrown away at a restart).
+// The replacement residual is formed in the scaled basis from the FP64 W blocks,
+// r^ = r^_0 + (I + F^) lam^; the stopping test always uses an exact gamma - S lam.
 
 
 template <class T>
@@ -843,11 +846,21 @@ __device__ __forceinline__ float fhat_row(const float* __restrict__ w, int nx, i
   return a0 + a1;
 }
 
-// Any nx and horizon: thread rows g = tid + k*blockDim; five padded FP32 vectors
-// (K + 2 segments of ld floats with zero end segments) in shared memory, the W blocks
-// in shared or global memory.
+// Any nx and horizon: thread rows g = tid + k*blockDim; five padded FP32 vectors r^, p^, z^, u^, d^
+// (K + 2 segments of ld floats with zero end segments) in shared memory, the FP32 W blocks in
+// shared or global memory.  One FP32 PCG with FP64 residual replacement, by the same rules as
+// the compile-time row PCG (pcg_rows_scaled): the FP32 vectors carry the problem scaled by
+// 1/sqrt(eta64) of the first residual; each time the recursion's eta has fallen by `upd_rel`
+// (or rises 1e4-fold, or is not a number) the accumulated step goes into an FP64 sum lam^ (tmp),
+// the true scaled residual r^ = r^_0 + (I + F^) lam^ from the FP64 W blocks replaces the
+// recursive one and the search direction is kept; the convergence decision rests on an exact
+// residual gamma - S lam (evaluated once the recursion is below 0.1 eps, or when the replaced
+// residual is).  The FP64 recurrence finishes the solve (fp64_finish) when a replacement that the
+// recursion's fall (or the stall detection) triggered shows a true fall of less than 100x, after
+// max_ref replacements, after half the budget, or on a non-finite recursion.  FP64 vectors in workspace regions free
+// during the solve: r^_0 t1, candidate r^ xn, z^ (FP64) C, lam^ tmp.
 __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, float* vec, int max_iter, double eps,
-                                                int max_ref, double inner_rel, double* red, int& par) {
+                                                int max_ref, double upd_rel, double* red, int& par) {
   const int nx = s.nx, N = s.N, K = s.K, ld = s.ld, n = K * nx;
   const int span = (K + 2) * ld;
   for (int w = threadIdx.x; w < 5 * span; w += blockDim.x) vec[w] = 0.f;
@@ -857,87 +870,164 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
   float* uv = zv + span;
   float* dv = uv + span;
   const float* w32 = s.w32;
-  int it = 0;
-  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
-  double eta64 = 0.0, prev64 = 0.0;
-  for (int ref = 0;; ++ref) {
-    // res = gamma - S lam, r^ = L^-1 res (t1), eta64 = r^T (I - F^) r^ = res^T Phi^-1 res
+  const double* w64 = s.pm;  // FP64 W blocks (row stride nx, block N zero)
+  double *rh0 = s.t1, *rhc = s.xn, *zh = s.C, *acc = s.tmp;
+  const int w2 = warp_pow2();
+  // res = gamma - S lam, r^_0 = L^-1 res (t1)
+  auto exact = [&]() {
     for (int g = threadIdx.x; g < n; g += blockDim.x)
       s.res[g] = s.gam[g] + stencil_row<double, double>(s.th, s.ph, nx, nx, N, lam, g);
     __syncthreads();
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
       const int t = g / nx;
-      s.t1[g] = lower_row(s.li, nx, t, g - t * nx, s.res);
+      rh0[g] = lower_row(s.li, nx, t, g - t * nx, s.res);
     }
     __syncthreads();
+  };
+  // z^ = r^ - F^ r^ in FP64 (zh) for an FP64 r^; returns eta64 = r^.z^
+  auto eta_of = [&](const double* rh) -> double {
     double part = 0.0;
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
       const int t = g / nx;
-      part += s.t1[g] * (s.t1[g] - fhat64_row(s.pm, nx, N, t, g - t * nx, s.t1));
+      const double z = rh[g] - fhat64_row(w64, nx, N, t, g - t * nx, rh);
+      zh[g] = z;
+      part += rh[g] * z;
     }
-    eta64 = block_sum(part, red, par);
-    const bool cont = (fabs(eta64) > eps && it <= max_iter - 1) || it < 1;
-    if (!cont || !(eta64 == eta64)) break;
-    if (ref >= max_ref || it >= it_cap || (ref > 0 && eta64 > kStagnation * prev64))
-      return fp64_finish(s, lam, it, max_iter, eps, red, par);
-    prev64 = eta64;
-    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+    return block_sum(part, red, par);
+  };
+  // lam += L^-T lam^, lam^ = 0
+  auto flush = [&]() {
+    __syncthreads();
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
-      const int t = g / nx, i = g - t * nx, x = t * ld + i;
-      rv[x] = (float)(scale * s.t1[g]);
-      dv[x] = 0.f;
+      const int t = g / nx;
+      zh[g] = lower_col64(s.li, nx, t, g - t * nx, acc + (size_t)t * nx);
     }
     __syncthreads();
-    part = 0.0;
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
-      const int t = g / nx, i = g - t * nx, x = t * ld + i;
-      const float z = rv[x] - fhat_row(w32, nx, ld, N, t, i, rv);
-      pv[x] = z;
-      part += (double)rv[x] * (double)z;
+      lam[g] += zh[g];
+      acc[g] = 0.0;
     }
-    double eta = block_sum(part, red, par);
-    const double target = fmax(inner_rel * eta, eps * scale * scale * 0.01);
-    int inner = 0;
-    while ((eta > target && it < it_cap) || inner < 1) {
-      part = 0.0;
+    __syncthreads();
+  };
+  // scaled FP32 copies of an FP64 r^ (and of zh)
+  auto load32 = [&](const double* rh, double scale) {
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx, x = t * ld + (g - t * nx);
+      rv[x] = (float)(scale * rh[g]);
+      zv[x] = (float)(scale * zh[g]);
+    }
+  };
+  for (int g = threadIdx.x; g < n; g += blockDim.x) acc[g] = 0.0;
+  exact();
+  double eta64 = eta_of(rh0);
+  int it = 0;
+  if (!(eta64 == eta64)) return PcgOut{it, eta64};  // the reference loop always runs an iteration
+  const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0, back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+  const double s2 = scale * scale, check_at = eps * s2 * kCheckMargin;
+  double prev64 = eta64, eta_upd = eta64 * s2, eta = eta64 * s2;
+  int nupd = 0, seg0 = 0;
+  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
+  int it_stop = min(it_cap, kStallMin);  // stall detection: the current segment ends here at the latest
+  load32(rh0, scale);
+  __syncthreads();
+  for (int g = threadIdx.x; g < n; g += blockDim.x) {
+    const int t = g / nx, x = t * ld + (g - t * nx);
+    pv[x] = zv[x];
+  }
+  double trig = fmax(check_at, upd_rel * eta), hi = kDivergeRatio * eta;
+  __syncthreads();
+  for (;;) {
+    double vden, etap;
+    for (;;) {
+      // u^ = S^ p^ = -(p^ + F^ p^)
+      float part = 0.f;
       for (int g = threadIdx.x; g < n; g += blockDim.x) {
         const int t = g / nx, i = g - t * nx, x = t * ld + i;
         const float u = -(pv[x] + fhat_row(w32, nx, ld, N, t, i, pv));
         uv[x] = u;
-        part += (double)pv[x] * (double)u;
+        part = fmaf(pv[x], u, part);
       }
-      const double vden = block_sum(part, red, par);
-      const float alpha = (float)(eta / vden);
+      vden = block_sum_f32w(part, red, par, w2);
+      const float alpha = quot32(eta, vden);
       for (int g = threadIdx.x; g < n; g += blockDim.x) {
         const int t = g / nx, x = t * ld + (g - t * nx);
         dv[x] = fmaf(alpha, pv[x], dv[x]);
         rv[x] = fmaf(-alpha, uv[x], rv[x]);
       }
       __syncthreads();
-      part = 0.0;
+      // z^ = Phi^ r^ = r^ - F^ r^
+      part = 0.f;
       for (int g = threadIdx.x; g < n; g += blockDim.x) {
         const int t = g / nx, i = g - t * nx, x = t * ld + i;
         const float z = rv[x] - fhat_row(w32, nx, ld, N, t, i, rv);
         zv[x] = z;
-        part += (double)rv[x] * (double)z;
+        part = fmaf(rv[x], z, part);
       }
-      const double etap = block_sum(part, red, par);
-      const float beta = (float)(etap / eta);
+      etap = block_sum_f32w(part, red, par, w2);
+      ++it;
+      if (!(etap > trig) || etap > hi || it >= it_stop || !(vden == vden)) break;
+      const float beta = quot32(etap, eta);
       for (int g = threadIdx.x; g < n; g += blockDim.x) {
         const int t = g / nx, x = t * ld + (g - t * nx);
         pv[x] = fmaf(beta, pv[x], zv[x]);
       }
       eta = etap;
-      ++it;
-      ++inner;
       __syncthreads();
-      if (!(eta == eta) || !(vden == vden)) break;
     }
-    const double back = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+    // Residual replacement (see above); a non-finite segment is dropped.
+    const bool bad = !(etap == etap) || !(vden == vden);
+    const bool at_check = etap <= check_at;
+    const bool progressed = etap <= upd_rel * eta_upd || etap > hi || (it >= it_stop && it < it_cap);
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
-      const int t = g / nx, i = g - t * nx;
-      lam[g] += back * lower_col(s.li, nx, t, i, dv + t * ld);
+      const int t = g / nx, x = t * ld + (g - t * nx);
+      if (!bad) acc[g] += back * (double)dv[x];
+      dv[x] = 0.f;
     }
+    __syncthreads();
+    bool exact_now = bad || at_check || it >= it_cap;
+    const double* rh = rh0;
+    if (!exact_now) {
+      for (int g = threadIdx.x; g < n; g += blockDim.x) {
+        const int t = g / nx;
+        rhc[g] = rh0[g] + acc[g] + fhat64_row(w64, nx, N, t, g - t * nx, acc);
+      }
+      __syncthreads();
+      eta64 = eta_of(rhc);
+      rh = rhc;
+      exact_now = !(eta64 > eps);
+    }
+    if (exact_now) {
+      flush();
+      exact();
+      eta64 = eta_of(rh0);
+      rh = rh0;
+    }
+    ++nupd;
+    if (!(fabs(eta64) > eps && it <= max_iter - 1) || !(eta64 == eta64)) {
+      if (!exact_now) flush();
+      break;
+    }
+    const double etas = eta64 * s2;
+    if (bad || nupd >= max_ref || it >= it_cap || !(etas > 0.0) ||
+        (progressed && !at_check && eta64 > kUpdateStagnation * prev64)) {
+      if (!exact_now) flush();
+      return fp64_finish(s, lam, it, max_iter, eps, red, par);
+    }
+    prev64 = eta64;
+    eta_upd = etas;
+    it_stop = next_stop(it, it - seg0, it_cap);
+    seg0 = it;
+    load32(rh, scale);
+    const bool restart = etas > kRestartRatio * eta;  // a stale direction: restart it
+    const float beta = restart ? 0.f : quot32(etas, eta);
+    __syncthreads();
+    for (int g = threadIdx.x; g < n; g += blockDim.x) {
+      const int t = g / nx, x = t * ld + (g - t * nx);
+      pv[x] = fmaf(beta, pv[x], zv[x]);
+    }
+    eta = etas;
+    trig = fmax(check_at, upd_rel * etas);
+    hi = kDivergeRatio * etas;
     __syncthreads();
   }
   return PcgOut{it, eta64};
@@ -1104,7 +1194,8 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
     // The FP32 vectors carry the problem scaled by 1/sqrt(eta64) of the first residual
     // (eta starts at 1) and keep that scale through every replacement.  cst: scale,
     // sqrt(eta64_0), scale^2, the convergence-check level, eta64 and the scaled eta at the
-    // last replacement, eps, upd_rel, max_ref, the replacement count, max_iter.
+    // last replacement, eps, upd_rel, max_ref, the replacement count, max_iter, the first
+    // iteration of the current FP32 segment.
     const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
     double* cst = x64_of() + (K + 1) * NX;
     if (threadIdx.x == 0) {
@@ -1119,6 +1210,7 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
       cst[8] = (double)max_ref;
       cst[9] = 0.0;
       cst[10] = (double)max_iter;
+      cst[11] = 0.0;
     }
 #pragma unroll
     for (int k = 0; k < R; ++k) {
@@ -1131,7 +1223,9 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
     trig = (float)fmax(eps * scale * scale * kCheckMargin, upd_rel * eta);
     hi = (float)(kDivergeRatio * eta);
   }
-  const int it_cap = max_iter / 2;  // FP32 share of the budget; the rest is kept for fp64_finish
+  // the FP32 segment ends at it_stop at the latest (stall detection; max_iter / 2, the FP32 share
+  // of the budget, bounds it: the rest is kept for fp64_finish)
+  int it_stop = min(max_iter / 2, kStallMin);
   store(pv, p);
   __syncthreads();
   double eta64 = 0.0;
@@ -1177,7 +1271,7 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
         etap = block_sum_f32w(dot32(r, z), red, par, w2);
         ++it;
         const float etaf = (float)etap;
-        if (!(etaf > trig) || etaf > hi || it >= it_cap || !(vden == vden)) break;
+        if (!(etaf > trig) || etaf > hi || it >= it_stop || !(vden == vden)) break;
         const float beta = quot32(etap, eta);
 #pragma unroll
         for (int k = 0; k < R; ++k) p[k] = fmaf(beta, p[k], z[k]);
@@ -1195,10 +1289,11 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
       double* acc = s.tmp;
       const double scale = cst[0], back = cst[1], s2 = cst[2], check_at = cst[3], prev64 = cst[4],
                    eta_upd = cst[5], c_eps = cst[6], c_upd = cst[7];
-      const int c_maxref = (int)cst[8], nupd = (int)cst[9] + 1, c_maxit = (int)cst[10];
+      const int c_maxref = (int)cst[8], nupd = (int)cst[9] + 1, c_maxit = (int)cst[10], it_cap = c_maxit / 2;
       const bool bad = !(etap == etap) || !(vden == vden);
       const bool at_check = etap <= check_at;
-      const bool progressed = etap <= c_upd * eta_upd || (float)etap > hi;
+      // a segment cut by the stall detection counts as progress for the stagnation rule
+      const bool progressed = etap <= c_upd * eta_upd || (float)etap > hi || (it >= it_stop && it < it_cap);
       // a non-finite segment is dropped: lam keeps the last finite update
       double a[R];
 #pragma unroll
@@ -1242,10 +1337,13 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
         if (!exact) flush();
         return fp64_finish(s, lam, it, c_maxit, c_eps, red, par);
       }
+      it_stop = next_stop(it, it - (int)cst[11], it_cap);
+      __syncthreads();
       if (threadIdx.x == 0) {
         cst[4] = eta64;
         cst[5] = etas;
         cst[9] = (double)nupd;
+        cst[11] = (double)it;
       }
 #pragma unroll
       for (int k = 0; k < R; ++k) {

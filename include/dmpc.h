@@ -106,12 +106,13 @@ typedef struct dmpc_solver_params {
                                      an FP64 fallback recurrence then gets a full budget of its own */
   double pcg_tol_epsilon;         /* sqp.yaml pcg.tol_epsilon (absolute, on eta = r^T Phi^-1 r) */
   int32_t precision;              /* DMPC_PREC_* */
-  int32_t max_refinement;         /* MIXED: FP64 residual evaluations per QP solve (replacements in the
-                                     row-pair PCG, restarts otherwise) before the FP64 fallback */
+  int32_t max_refinement;         /* MIXED: FP64 residual replacements per QP solve before the FP64
+                                     fallback */
   double inner_rel_tol;           /* MIXED: the FP32 recursion's eta falls by this factor between FP64
-                                     residual replacements (row-pair PCG) or restarts (other nx) */
-  int32_t threads_per_block;      /* 0 = automatic: one thread per row pair of the FP32 PCG (else per row),
-                                     256..512; or 64..512, a multiple of 32 (diffmpc_b200.autotune) */
+                                     residual replacements */
+  int32_t threads_per_block;      /* 0 = automatic: one thread per knot and row quadruple of the FP32 PCG
+                                     (else per row), 256..512; or 64..512, a multiple of 32, within the
+                                     cta_config's limit (diffmpc_b200.autotune) */
   int32_t blocks_in_smem;         /* MIXED, the FP32 scaled off-diagonal blocks: -1 shared memory when they
                                      fit (per instance in a ragged group), 0 workspace, 1 require shared */
   int32_t cta_config;             /* DMPC_CTA_*: CTA shape of the solver kernels (diffmpc_b200.autotune) */

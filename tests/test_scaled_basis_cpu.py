@@ -5,9 +5,13 @@ rests on, using the oracle's S and Phi^-1 (pcg.py:160-243):
 * L^T Phi^-1 L = I - F^ and L^-1 S L^-T = -(I + F^), with F^ zero on the block diagonal;
 * PCG on (S^, I - F^) from r^ = L^-1 r produces the reference recurrence's eta sequence
   and, mapped back by L^-T, its iterates;
-* the two mixed-precision recurrences of the kernels, restated in numpy with FP32 vectors
-  (residual replacement on the row-pair path, restarting refinement elsewhere), stop on the
-  reference's FP64 test and reach the solution; replacement needs fewer FP32 iterations.
+* the kernels' mixed-precision recurrence (FP32 PCG with FP64 residual replacement and stall
+  detection, sqp_device.cuh: pcg_rows_scaled and pcg_mixed_scaled), restated in numpy with FP32
+  vectors, stops on the reference's FP64 test and reaches the solution; it needs fewer FP32
+  iterations than restarting refinement, which at the shipped inner tolerance (1e-3) cannot
+  meet a 1e4-fold stagnation rule and would hand every solve to the FP64 recurrence;
+* on ill-conditioned systems the stall detection hands the solve to the FP64 recurrence after
+  a few hundred FP32 iterations instead of half the budget.
 """
 
 import numpy as np
@@ -100,14 +104,21 @@ def _fp64_finish(Sd, Pd, gam, lam, eps, max_iter):
     return lam, it, e
 
 
-def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_iter=10000, Pd=None, max_ref=30):
-    """Numpy restatement of the row-pair kernel's mixed recurrence (solver.cu, pcg_pair_scaled):
-    FP32 vectors and FP32 F^, FP64 dot products, and the FP32 residual replaced by the FP64 one,
-    r^ = r^_0 + (I + F^) lam^, each time the recursion's eta falls by `upd_rel`; convergence is
-    decided on an exact residual gamma - S lam.  With Pd given, the kernel's hand-over rules
-    apply (a recursion-triggered replacement whose true eta fell by less than 100x, a diverging
-    recursion, half the budget or max_ref replacements spent) and the FP64 recurrence finishes;
-    the replacement count is then returned negated.  Returns (lam, iterations, replacements, eta64)."""
+STALL_MIN, STALL_GROWTH = 200, 4  # sqp_device.cuh: kStallMin, kStallGrowth
+
+
+def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_iter=10000, Pd=None, max_ref=30,
+                     stall=True, stats=None):
+    """Numpy restatement of the kernels' mixed recurrence (sqp_device.cuh: pcg_rows_scaled,
+    pcg_mixed_scaled): FP32 vectors and FP32 F^, FP64 dot products, and the FP32 residual replaced
+    by the FP64 one, r^ = r^_0 + (I + F^) lam^, each time the recursion's eta falls by `upd_rel`;
+    convergence is decided on an exact residual gamma - S lam.  With `stall`, an FP32 segment is
+    also cut after max(4 x the previous segment, 200) iterations (200 for the first).  With Pd
+    given, the kernels' hand-over rules apply (a replacement triggered by the recursion's fall, by
+    its divergence or by the stall cut whose true eta fell by less than 100x; half the budget or
+    max_ref replacements spent) and the FP64 recurrence finishes; the replacement count is then
+    returned negated and, with `stats` (a dict), the FP64 iteration count stored under "fp64".
+    Returns (lam, iterations, replacements, eta64)."""
     f32, f64 = np.float32, np.float64
     F64 = Fh
     F32 = Fh.astype(f32)
@@ -125,7 +136,9 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
     trig = max(check_at, upd_rel * eta)
     hi = 1e4 * eta
     eta_upd, prev64 = eta, eta64
-    it = nrep = 0
+    it = nrep = seg0 = 0
+    it_cap = max_iter // 2
+    it_stop = min(it_cap, STALL_MIN) if stall else it_cap
     while True:
         u = -(p + F32 @ p)
         vden = float(p.astype(f64) @ u.astype(f64))
@@ -135,14 +148,14 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
         z = r - F32 @ r
         etap = float(r.astype(f64) @ z.astype(f64))
         it += 1
-        if trig < etap <= hi and it < max_iter // 2:
+        if trig < etap <= hi and it < it_stop:
             p = z + f32(etap / eta) * p
             eta = etap
             continue
         acc = acc + d.astype(f64) / scale
         d = np.zeros_like(r)
         at_check = etap <= check_at
-        progressed = etap <= upd_rel * eta_upd or etap > hi
+        progressed = etap <= upd_rel * eta_upd or etap > hi or it_stop <= it < it_cap
         exact = at_check
         if not exact:
             rh = rh0 + acc + F64 @ acc
@@ -159,11 +172,16 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
             return lam + Li.T @ acc, it, nrep, eta64
         etas = eta64 * s2
         stalled = progressed and not at_check and eta64 > 1e-2 * prev64
-        if Pd is not None and (it >= max_iter // 2 or nrep >= max_ref or stalled):
+        if Pd is not None and (it >= it_cap or nrep >= max_ref or stalled):
             lam, it64, e = _fp64_finish(Sd, Pd, gam, lam + Li.T @ acc, eps, max_iter)
+            if stats is not None:
+                stats["fp64"] = it64
             return lam, it + it64, -nrep, e
-        assert it < max_iter // 2, "FP32 share of the budget exhausted"
+        assert it < it_cap, "FP32 share of the budget exhausted"
         eta_upd, prev64 = etas, eta64
+        if stall:
+            it_stop = min(it_cap, it + max(STALL_GROWTH * (it - seg0), STALL_MIN))
+        seg0 = it
         r = (scale * rh).astype(f32)
         z = (scale * (rh - F64 @ rh)).astype(f32)
         if etas > 10.0 * eta:
@@ -174,19 +192,26 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
         hi = 1e4 * etas
 
 
-def _pcg_restart(Fh, Li, Sd, gam, eps, inner_rel=1e-8, max_ref=30):
-    """Numpy restatement of the generic mixed path (solver.cu, pcg_mixed_scaled): FP64
-    iterative refinement around FP32 PCG solves that restart from the scaled FP64 residual
-    and stop at inner_rel * eta (or 0.01 eps).  Returns (lam, iterations, refinements, eta64)."""
+def _pcg_restart(Fh, Li, Sd, gam, eps, inner_rel=1e-3, max_ref=30, stagnation=1e-4, Pd=None):
+    """Restarting refinement, the alternative to residual replacement: FP64 iterative refinement
+    around FP32 PCG solves that restart from the scaled FP64 residual and stop at inner_rel * eta
+    (or 0.01 eps).  With Pd given, a refinement that cuts eta64 by less than 1/stagnation, or the
+    max_ref-th refinement, hands the solve to the FP64 recurrence and the refinement count is
+    returned negated.  Returns (lam, iterations, refinements, eta64)."""
     f32, f64 = np.float32, np.float64
     F32 = Fh.astype(f32)
     lam = np.zeros_like(gam)
     it = 0
-    for ref in range(max_ref):
+    prev64 = None
+    for ref in range(max_ref + 1):
         rh = Li @ (gam - Sd @ lam)
         eta64 = float(rh @ (rh - Fh @ rh))
         if not abs(eta64) > eps:
             return lam, it, ref, eta64
+        if Pd is not None and (ref >= max_ref or (prev64 is not None and eta64 > stagnation * prev64)):
+            lam, it64, e = _fp64_finish(Sd, Pd, gam, lam, eps, 10000)
+            return lam, it + it64, -ref, e
+        prev64 = eta64
         scale = 1.0 / np.sqrt(eta64)
         r = (scale * rh).astype(f32)
         d = np.zeros_like(r)
@@ -208,72 +233,82 @@ def _pcg_restart(Fh, Li, Sd, gam, eps, inner_rel=1e-8, max_ref=30):
     raise AssertionError("refinement did not converge")
 
 
+def _scaled(seed, qspread=2.0):
+    S, Phi, gam, K, nx = _system(seed, qspread=qspread)
+    Sd, Pd = _dense(S, K, nx).numpy(), _dense(Phi, K, nx).numpy()
+    n = K * nx
+    L = np.zeros((n, n))
+    for t in range(K):
+        L[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx] = np.linalg.cholesky(-Sd[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx])
+    Li = np.linalg.inv(L)
+    Fh = -(Li @ Sd @ Li.T) - np.eye(n)
+    return Sd, Pd, gam.numpy(), Li, Fh
+
+
 def test_mixed_recurrences_reach_the_fp64_stopping_rule():
     """Both mixed recurrences stop only on an exact FP64 eta below eps and reach the solution
     of S lam = gamma to the accuracy that eps allows.  Keeping the search direction across the
-    FP64 corrections (residual replacement) takes fewer FP32 iterations than restarting at each
-    refinement, as measured on the GPU (quadrotor QPs: 327 vs 424 per QP, FP64 PCG 256)."""
+    FP64 corrections (residual replacement, at the shipped defaults) takes fewer FP32 iterations
+    than restarting at each refinement, even when the restarted inner solves run to 1e-8."""
     for seed in (0, 1, 2):
-        S, Phi, gam, K, nx = _system(seed)
-        Sd, Pd = _dense(S, K, nx).numpy(), _dense(Phi, K, nx).numpy()
-        g = gam.numpy()
-        n = K * nx
-        L = np.zeros((n, n))
-        for t in range(K):
-            L[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx] = np.linalg.cholesky(-Sd[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx])
-        Li = np.linalg.inv(L)
-        Fh = -(Li @ Sd @ Li.T) - np.eye(n)
+        Sd, Pd, g, Li, Fh = _scaled(seed)
+        n = g.shape[0]
         exact = np.linalg.solve(Sd, g)
         eps = 1e-22 * float(g @ g)
         its = {}
-        for name, solve in (("replace", _pcg_replacement), ("restart", _pcg_restart)):
+        for name, solve in (("replace", _pcg_replacement),
+                            ("restart", lambda *a: _pcg_restart(*a, inner_rel=1e-8))):
             lam, it, nfix, eta64 = solve(Fh, Li, Sd, g, eps)
             res = g - Sd @ lam
             assert float(res @ (Pd @ res)) <= eps, name
             assert abs(eta64 - float(res @ (Pd @ res))) <= 1e-6 * eps + 1e-12 * abs(eta64), name
             assert np.abs(lam - exact).max() <= 1e-8 * np.abs(exact).max(), name
-            assert nfix <= 30, name
+            assert 0 < nfix <= 30, name
             its[name] = it
-        # the FP64 reference recurrence to the same eps
-        x, rr = np.zeros(n), g.copy()
-        zz = Pd @ rr
-        pp, e = zz.copy(), float(rr @ zz)
-        it64 = 0
-        while abs(e) > eps or it64 < 1:
-            uu = Sd @ pp
-            a = e / float(pp @ uu)
-            x, rr = x + a * pp, rr - a * uu
-            zz = Pd @ rr
-            e2 = float(rr @ zz)
-            pp, e = zz + (e2 / e) * pp, e2
-            it64 += 1
+        _, it64, _ = _fp64_finish(Sd, Pd, g, np.zeros(n), eps, 10000)
         assert its["replace"] < its["restart"], (seed, its)
         assert its["replace"] <= 2.5 * it64, (seed, its, it64)
 
 
+def test_restarting_refinement_at_the_shipped_tolerance_always_hands_over():
+    """An FP32 inner solve stopped at the shipped relative tolerance (1e-3) cuts eta64 by about
+    1e3, never by the 1e4 a restarting scheme's stagnation rule asks for, so restarting refinement
+    with those settings would hand every solve to the FP64 recurrence after one refinement.
+    Residual replacement at the same settings (a 100-fold true fall per 1e3-fold recursion fall)
+    finishes these systems in FP32 with no hand-over."""
+    for seed in (0, 1, 2):
+        Sd, Pd, g, Li, Fh = _scaled(seed)
+        eps = 1e-20 * float(g @ g)
+        _, _, nref, eta = _pcg_restart(Fh, Li, Sd, g, eps, inner_rel=1e-3, stagnation=1e-4, Pd=Pd)
+        assert nref == -1, (seed, nref)  # handed over after the first refinement
+        assert abs(eta) <= eps
+        _, _, nrep, eta = _pcg_replacement(Fh, Li, Sd, g, eps, upd_rel=1e-3, Pd=Pd)
+        assert nrep > 0, (seed, nrep)
+        assert abs(eta) <= eps
+
+
 def test_ill_conditioned_systems_hand_over_to_fp64_and_match_the_reference_recurrence():
     """Diagonal cost weights over 1e-6..1e6 (cond(S) 1e10..1e11, the precision-stress shape):
-    the FP32 recursion stalls, the hand-over rules send the solve to the FP64 recurrence, which
-    ends on the reference's stopping test, and the solution is as accurate as that of the
-    reference recurrence run alone to the same eps.  (At this conditioning the recursively
-    updated eta of either drifts above the true one, so the true eta is not compared.)"""
-    handed_over = 0
+    the FP32 recursion stalls, the stall detection cuts its segment and the stagnation rule sends
+    the solve to the FP64 recurrence, which ends on the reference's stopping test; the solution is
+    as accurate as that of the reference recurrence run alone to the same eps.  Without the stall
+    detection the FP32 recursion runs to half the budget (5000 iterations) first.  (At this
+    conditioning the recursively updated eta of either drifts above the true one, so the true eta
+    is not compared.)"""
     for seed in (3, 4, 5):
-        S, Phi, gam, K, nx = _system(seed, qspread=6.0)
-        Sd, Pd = _dense(S, K, nx).numpy(), _dense(Phi, K, nx).numpy()
-        g = gam.numpy()
-        n = K * nx
-        L = np.zeros((n, n))
-        for t in range(K):
-            L[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx] = np.linalg.cholesky(-Sd[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx])
-        Li = np.linalg.inv(L)
-        Fh = -(Li @ Sd @ Li.T) - np.eye(n)
+        Sd, Pd, g, Li, Fh = _scaled(seed, qspread=6.0)
+        n = g.shape[0]
         eps = 1e-20 * float(g @ g)
         exact = np.linalg.solve(Sd, g)
         ref, _, _ = _fp64_finish(Sd, Pd, g, np.zeros(n), eps, 10000)
-        lam, it, nrep, eta = _pcg_replacement(Fh, Li, Sd, g, eps, Pd=Pd)
+        st = {}
+        lam, it, nrep, eta = _pcg_replacement(Fh, Li, Sd, g, eps, Pd=Pd, stats=st)
+        assert nrep < 0, (seed, nrep)
         assert abs(eta) <= eps, (seed, nrep, eta)
         err, rerr = np.abs(lam - exact).max(), np.abs(ref - exact).max()
         assert err <= 10.0 * rerr + 1e-9 * np.abs(exact).max(), (seed, err, rerr)
-        handed_over += nrep < 0
-    assert handed_over >= 2
+        fp32_its = it - st["fp64"]
+        assert fp32_its <= 2 * STALL_MIN + 100, (seed, fp32_its)
+        st_off = {}
+        _, it_off, nrep_off, _ = _pcg_replacement(Fh, Li, Sd, g, eps, Pd=Pd, stall=False, stats=st_off)
+        assert nrep_off < 0 and it_off - st_off["fp64"] >= 3000, (seed, it_off, st_off)
