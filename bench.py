@@ -246,6 +246,29 @@ def _sqp_stats(sol):
             "pcg_iters_per_instance": float(sol.num_pcg_iters.double().sum() / sol.status.numel())}
 
 
+def precision_record(solver, sol):
+    """What the FP64 corrections of the mixed PCG did in the solver's last step: FP64 residual
+    replacements per QP solve, the QP solves the FP32 PCG handed to the FP64 recurrence, and the
+    FP64 recurrence's share of all PCG iterations (forward QPs, and the adjoint QP)."""
+    import torch
+
+    rec = solver.last_forward_pcg_record
+    if rec is None:
+        return None
+    mi = rec.shape[-1]
+    ran = torch.arange(mi, device=rec.device)[None, :] < sol.num_iter.to(rec.device).long()[:, None]
+    corr, f64 = rec[0][ran].double(), rec[1][ran].double()
+    its = sol.num_pcg_iters.to(rec.device)[ran].double()
+    out = {"qp_solves": int(ran.sum()), "replacements_per_qp": float(corr.mean()),
+           "qp_handed_to_fp64": int((f64 > 0).sum()), "fp64_iter_share": float(f64.sum() / its.sum().clamp_min(1))}
+    a, ai = solver.last_adjoint_pcg_record, solver.last_adjoint_pcg_iters
+    if a is not None and ai is not None:
+        out["adjoint"] = {"qp_solves": int(a.shape[1]), "replacements_per_qp": float(a[0].double().mean()),
+                          "qp_handed_to_fp64": int((a[1] > 0).sum()),
+                          "fp64_iter_share": float(a[1].double().sum() / ai.double().sum().clamp_min(1))}
+    return out
+
+
 def parity_block(sp, dyn, st, p, sol, grads):
     """Parity of the timed mixed-precision result over the whole batch against the all-FP64 path
     (the reference recurrence, same parameters).  Two FP64-vs-FP64 controls stand beside it for
@@ -490,6 +513,7 @@ def run_ours(args):
             "l2": "512 MB buffer written between timed steps; solver workspace one slot per resident CTA",
         },
         "roofline": roofline, "clocks": clocks, "gpu_launches": gpu_launches,
+        "precision_record": precision_record(solver, sol),
     }
 
     if not args.no_extras:
@@ -753,7 +777,7 @@ def run_other_workload(args):
                                   "diffmpc_TFRT_CPU_0_{fwd,bwd}.npy (median)"},
                     pcg_iters_per_solve=float(roll.last.pcg_hist.double().sum() / (B * T)))
     else:  # stress
-        B = args.batch if args.batch != 4096 else 1024
+        B = args.batch if args.batch != 4096 else 16384
         dyn, st, bt, sp = workloads.linear_stress(B=B)
         sp["pcg"]["tol_epsilon"] = args.pcg_tol
         sp["num_scp_iteration_max"] = 2
@@ -772,13 +796,16 @@ def run_other_workload(args):
 
             ms, (sol, w) = _timed(step, args.steps, args.warmup)
             out[prec] = (ms, sol.controls.detach().cpu(), w["weights_penalization_reference_state_trajectory"].grad.cpu(),
-                         sol.num_pcg_iters.sum(dim=1).double().mean().item())
+                         sol.num_pcg_iters.sum(dim=1).double().mean().item(), precision_record(solver, sol))
         c64, g64 = out["fp64"][1], out["fp64"][2]
         line.update(metric="fwd+bwd MPC solves/s, linear nx=24 nu=8 N=128, diag Q 1e-3..1e3, B=%d" % B,
                     value=B / (out["mixed"][0] * 1e-3), fp64_value=B / (out["fp64"][0] * 1e-3),
                     max_rel_control_diff_mixed_vs_fp64=float((out["mixed"][1] - c64).abs().max() / c64.abs().max()),
                     max_rel_grad_diff_mixed_vs_fp64=float((out["mixed"][2] - g64).abs().max() / g64.abs().max()),
-                    pcg_iters_mixed=out["mixed"][3], pcg_iters_fp64=out["fp64"][3])
+                    controls_mixed_vs_fp64=_dist(_rel_per_instance(out["mixed"][1], c64), 1e-6),
+                    grads_mixed_vs_fp64=_dist(_rel_per_instance(out["mixed"][2], g64), 1e-5),
+                    pcg_iters_mixed=out["mixed"][3], pcg_iters_fp64=out["fp64"][3],
+                    refinement_steps=out["mixed"][4]["replacements_per_qp"], precision_record=out["mixed"][4])
     print(json.dumps(line), flush=True)
 
 

@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdmpc.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 DMPC_OK = 0
 DMPC_ERR_CUDA = 3
 DMPC_MAX_NX = 32
@@ -102,6 +102,8 @@ class Group(ctypes.Structure):
         ("num_pcg_iters", _p),
         ("lin_states", _p),
         ("lin_controls", _p),
+        ("num_pcg_corrections", _p),
+        ("num_pcg_fp64_iters", _p),
     ]
 
 
@@ -124,6 +126,8 @@ class Adjoint(ctypes.Structure):
         ("g_model_params", _p),
         ("adj_states", _p),
         ("adj_controls", _p),
+        ("num_pcg_corrections", _p),
+        ("num_pcg_fp64_iter", _p),
     ]
 
 

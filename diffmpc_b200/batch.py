@@ -44,6 +44,8 @@ class _GroupsFunction(torch.autograd.Function):
         _lib.check(lib.dmpc_solve_fwd(len(calls), groups, lead._c_params, ws.data_ptr(), ws.numel(), stream),
                    "dmpc_solve_fwd")
         lead._event_end(ev, "k_sqp_fwd")
+        for (solver, _, _, _), c in zip(problems, calls):
+            solver.last_forward_pcg_record = c.pcg_record
         holder["calls"] = calls
         ctx.problems, ctx.key_lists, ctx.calls, ctx.shapes, ctx.groups = problems, key_lists, calls, shapes, groups
         outs = []
@@ -75,6 +77,7 @@ class _GroupsFunction(torch.autograd.Function):
                    "dmpc_solve_adj")
         lead._event_end(ev, "k_sqp_adj")
         lead.last_adjoint_pcg_iters = [sp.adj_iters for sp in specs]
+        lead.last_adjoint_pcg_record = [sp.adj_record for sp in specs]
         out = [None, None, None]
         for spec, c, keys, shapes in zip(specs, ctx.calls, ctx.key_lists, ctx.shapes):
             g = spec.gradients()

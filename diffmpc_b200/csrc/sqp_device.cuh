@@ -522,8 +522,10 @@ __device__ __forceinline__ double stencil_row(const BT* Dg, const BT* Off, int l
 
 // ---------------------------------------------------------------- PCG, FP64 (reference recurrence)
 struct PcgOut {
-  int it;
+  int it;     // iterations (FP32 and FP64)
   double eta;
+  int nrep;   // FP64 residual replacements of the FP32 PCG
+  int it64;   // iterations of the FP64 recurrence
 };
 
 // Solves S lam = gam starting from lam (in/out, FP64 shared vector `lv`),
@@ -686,19 +688,18 @@ __device__ __noinline__ PcgOut pcg_fp64_scaled(const Inst& s, double* lam, int m
   return PcgOut{it, eta};
 }
 
-// FP32 refinement is not paying off: a refinement step cut eta64 by less than 1e4 (the
-// residual norm by less than 100x: kappa * eps32 is too close to 1 for the FP32 iterations
-// to reach their target in the true residual), or the FP32 iterations have used half of
-// pcg.max_iter.  Finish the solve with the FP64 recurrence (in the scaled basis, see
-// pcg_fp64_scaled).  The recurrence
-// gets the full pcg.max_iter budget of the reference's loop: the FP32 iterations before it
-// are cheaper and restart at every refinement, so they are not charged against it, and a
-// QP's reported iteration count can reach 1.5 max_iter.
-__device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, double eps, double* red, int& par) {
+// The FP32 PCG is not paying off (a replacement shows the true residual stalled while the
+// recursion fell, the recursion diverged or stalled, or the FP32 iterations used half of
+// pcg.max_iter or max_refinement replacements).  Finish the solve with the FP64 recurrence (in
+// the scaled basis, see pcg_fp64_scaled) from the current lam.  The recurrence gets the full
+// pcg.max_iter budget of the reference's loop: the FP32 iterations before it are cheaper and
+// not charged against it, so a QP's reported iteration count can reach 1.5 max_iter.
+__device__ PcgOut fp64_finish(const Inst& s, double* lam, int it, int max_iter, double eps, double* red, int& par,
+                              int nrep) {
   // without Cholesky factors (sh_scaled_bad) the reference-basis blocks theta^-1, P exist instead
   PcgOut o = sh_scaled_bad ? pcg_fp64(s, lam, s.res, s.t1, s.xn, s.C, max_iter, eps, red, par)
                            : pcg_fp64_scaled(s, lam, max_iter, eps, red, par);
-  return PcgOut{it + o.it, o.eta};
+  return PcgOut{it + o.it, o.eta, nrep, o.it};
 }
 // Residual-replacement PCGs (pcg_rows_scaled, pcg_mixed_scaled): the FP64 convergence test runs once the
 // FP32 recursion's eta is below kCheckMargin * eps, and a replacement after which the
@@ -1011,7 +1012,7 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
     if (bad || nupd >= max_ref || it >= it_cap || !(etas > 0.0) ||
         (progressed && !at_check && eta64 > kUpdateStagnation * prev64)) {
       if (!exact_now) flush();
-      return fp64_finish(s, lam, it, max_iter, eps, red, par);
+      return fp64_finish(s, lam, it, max_iter, eps, red, par, nupd);
     }
     prev64 = eta64;
     eta_upd = etas;
@@ -1030,7 +1031,7 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
     hi = kDivergeRatio * etas;
     __syncthreads();
   }
-  return PcgOut{it, eta64};
+  return PcgOut{it, eta64, nupd};
 }
 
 // Compile-time nx, K ceil(nx / R) <= blockDim.  Thread (t, q) = (tid mod K, tid div K) owns the
@@ -1226,6 +1227,7 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
   // the FP32 segment ends at it_stop at the latest (stall detection; max_iter / 2, the FP32 share
   // of the budget, bounds it: the rest is kept for fp64_finish)
   int it_stop = min(max_iter / 2, kStallMin);
+  int nrep_out;  // set where the loop ends
   store(pv, p);
   __syncthreads();
   double eta64 = 0.0;
@@ -1329,13 +1331,14 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
       }
       if (!(fabs(eta64) > c_eps && it <= c_maxit - 1) || !(eta64 == eta64)) {
         if (!exact) flush();
+        nrep_out = nupd;
         break;
       }
       const double etas = eta64 * s2;
       if (bad || nupd >= c_maxref || it >= it_cap || !(etas > 0.0) ||
           (progressed && !at_check && eta64 > kUpdateStagnation * prev64)) {
         if (!exact) flush();
-        return fp64_finish(s, lam, it, c_maxit, c_eps, red, par);
+        return fp64_finish(s, lam, it, c_maxit, c_eps, red, par, nupd);
       }
       it_stop = next_stop(it, it - (int)cst[11], it_cap);
       __syncthreads();
@@ -1366,7 +1369,7 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
     eta = etap;
     __syncthreads();
   }
-  return PcgOut{it, eta64};
+  return PcgOut{it, eta64, nrep_out};
 }
 
 
@@ -1588,10 +1591,11 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
     PcgOut o = pcg_fp64(s, lv, rv, pv, tv, uv, P.pcg_max_iter, P.pcg_tol_epsilon, sv.red, par);
     for (int g = threadIdx.x; g < n; g += blockDim.x) lam[g] = lv[g];
     __syncthreads();
+    o.it64 = o.it;
     return o;
   }
   float* v = reinterpret_cast<float*>(sv.vec);
-  if (sh_scaled_bad) return fp64_finish(s, lam, 0, P.pcg_max_iter, P.pcg_tol_epsilon, sv.red, par);
+  if (sh_scaled_bad) return fp64_finish(s, lam, 0, P.pcg_max_iter, P.pcg_tol_epsilon, sv.red, par, 0);
   if (s.K * ((s.nx + 3) / 4) <= (int)blockDim.x) {
     switch (s.nx) {
 #define DMPC_ROWS(NXV)                                                                                   \
@@ -1680,6 +1684,8 @@ __device__ __forceinline__ void sqp_forward(const DevGroup& G, const dmpc_group&
     if (threadIdx.x == 0 && num_iter < maxit) {
       g.convergence_errors[(size_t)ii * maxit + num_iter] = conv_err;
       g.num_pcg_iters[(size_t)ii * maxit + num_iter] = o.it;
+      if (g.num_pcg_corrections) g.num_pcg_corrections[(size_t)ii * maxit + num_iter] = o.nrep;
+      if (g.num_pcg_fp64_iters) g.num_pcg_fp64_iters[(size_t)ii * maxit + num_iter] = o.it64;
       if (P.linesearch) g.linesearch_alphas[(size_t)ii * maxit + num_iter] = alpha;
     }
     for (int w = threadIdx.x; w < K * nx; w += blockDim.x) s.xb[w] = s.xn[w];
@@ -1767,6 +1773,8 @@ __device__ inline dmpc_group rollout_step_view(const dmpc_group& g0, const dmpc_
   v.convergence_errors = ra.step_convergence_errors + k * sh;
   v.linesearch_alphas = ra.step_linesearch_alphas + k * sh;
   v.num_pcg_iters = ra.step_num_pcg_iters + k * sh;
+  v.num_pcg_corrections = nullptr;
+  v.num_pcg_fp64_iters = nullptr;
   return v;
 }
 
@@ -1930,7 +1938,11 @@ __device__ __forceinline__ void sqp_adjoint(const DevGroup& G, const dmpc_group&
   }
   if (a.adj_controls)
     for (int w = threadIdx.x; w < K * nu; w += blockDim.x) a.adj_controls[ou + w] = ut[w];
-  if (threadIdx.x == 0 && a.num_pcg_iter) a.num_pcg_iter[ii] = o.it;
+  if (threadIdx.x == 0) {
+    if (a.num_pcg_iter) a.num_pcg_iter[ii] = o.it;
+    if (a.num_pcg_corrections) a.num_pcg_corrections[ii] = o.nrep;
+    if (a.num_pcg_fp64_iter) a.num_pcg_fp64_iter[ii] = o.it64;
+  }
   // closed-form gradients of the cost-related parameters (sqp.py:605-666,724-739)
   const int j = threadIdx.x;
   if (j < nx) {
@@ -2036,6 +2048,8 @@ __device__ __noinline__ void rollout_adj_instance(const DevArgs& args, const dmp
       a.dual_backward_guess = nullptr;  // the carried solution's backward guess is zero
       a.dual_backward = rr.scratch_dual;
       a.num_pcg_iter = nullptr;
+      a.num_pcg_corrections = nullptr;
+      a.num_pcg_fp64_iter = nullptr;
       a.g_initial_state = nullptr;
       a.adj_states = nullptr;
       a.adj_controls = nullptr;

@@ -153,6 +153,8 @@ class _Call:
         self.conv_hist = hist(guess.convergence_errors, torch.float64)
         self.alpha_hist = hist(guess.linesearch_alphas, torch.float64)
         self.pcg_hist = hist(guess.num_pcg_iters, torch.int32)
+        # per QP solve: FP64 residual replacements, and iterations of the FP64 recurrence
+        self.pcg_record = torch.zeros(2, B, mi, dtype=torch.int32, device=device)
         self.lin_states = torch.empty(B, K, nx, dtype=torch.float64, device=device)
         self.lin_controls = torch.empty(B, K, nu, dtype=torch.float64, device=device)
         g = _lib.Group()
@@ -170,6 +172,7 @@ class _Call:
         g.convergence_errors, g.linesearch_alphas = _ptr(self.conv_hist), _ptr(self.alpha_hist)
         g.num_pcg_iters = _ptr(self.pcg_hist)
         g.lin_states, g.lin_controls = _ptr(self.lin_states), _ptr(self.lin_controls)
+        g.num_pcg_corrections, g.num_pcg_fp64_iters = _ptr(self.pcg_record[0]), _ptr(self.pcg_record[1])
         self.group = g
 
 
@@ -188,8 +191,10 @@ class AdjointSpec:
         self.dbg = None if g_dbg is None else g_dbg.to(torch.float64).contiguous()
         self.dual_backward = z(B, K, nx)
         self.adj_iters = torch.zeros(B, dtype=torch.int32, device=dev)
+        self.adj_record = torch.zeros(2, B, dtype=torch.int32, device=dev)
         adj = _lib.Adjoint()
         adj.num_pcg_iter = self.adj_iters.data_ptr()
+        adj.num_pcg_corrections, adj.num_pcg_fp64_iter = self.adj_record[0].data_ptr(), self.adj_record[1].data_ptr()
         adj.dl_dstates, adj.dl_dcontrols = self.dlx.data_ptr(), self.dlu.data_ptr()
         adj.dual_backward_guess = _ptr(self.dbg)
         adj.dual_backward = self.dual_backward.data_ptr()
@@ -311,6 +316,12 @@ class SQPSolver:
         self.kernel_events = None
         # adjoint PCG iteration counts of the most recent backward pass, (B,) int32
         self.last_adjoint_pcg_iters = None
+        # precision record of the most recent forward solve, (2, B, num_scp_iteration_max) int32:
+        # [0] FP64 residual replacements of each QP's FP32 PCG, [1] iterations of the FP64
+        # recurrence (all of num_pcg_iters in FP64; > 0 in mixed precision when the FP32 PCG
+        # handed the QP over); and of the most recent backward pass, (2, B)
+        self.last_forward_pcg_record = None
+        self.last_adjoint_pcg_record = None
         self.solve = self._solve_differentiable
 
     # -- properties (sqp.py:100-133) ------------------------------------------
@@ -393,6 +404,7 @@ class SQPSolver:
         ev = self._event_pair()
         _lib.check(lib.dmpc_solve_fwd(1, call.group, self._c_params, ws.data_ptr(), ws.numel(), stream), "dmpc_solve_fwd")
         self._event_end(ev, "k_sqp_fwd")
+        self.last_forward_pcg_record = call.pcg_record
 
     def _event_pair(self):
         if self.kernel_events is None:
@@ -424,6 +436,7 @@ class SQPSolver:
             )
             self._event_end(ev, "k_sqp_adj")
         self.last_adjoint_pcg_iters = spec.adj_iters
+        self.last_adjoint_pcg_record = spec.adj_record
         return spec.gradients()
 
     # -- solve (sqp.py:436-560, 562-802) -------------------------------------------

@@ -53,7 +53,7 @@
 extern "C" {
 #endif
 
-#define DMPC_ABI_VERSION 2
+#define DMPC_ABI_VERSION 3
 
 /* return codes */
 #define DMPC_OK 0
@@ -160,6 +160,9 @@ typedef struct dmpc_group {
   int32_t* num_pcg_iters;          /* (batch, num_scp_iteration_max) in/out */
   double* lin_states;              /* (batch, K, nx) out: iterate of the last linearization */
   double* lin_controls;            /* (batch, K, nu) out */
+  /* precision record of each QP solve, optional (NULL: not written); (batch, num_scp_iteration_max) out */
+  int32_t* num_pcg_corrections;    /* FP64 residual replacements of the FP32 PCG (0 in FP64) */
+  int32_t* num_pcg_fp64_iters;     /* of num_pcg_iters, the iterations run by the FP64 recurrence */
 } dmpc_group;
 
 /* Adjoint inputs/outputs for one group (sqp.py:668-798).  Gradient outputs
@@ -183,6 +186,9 @@ typedef struct dmpc_adjoint {
   /* adjoint solution (x~, u~), optional (batch, K, nx) / (batch, K, nu) */
   double* adj_states;
   double* adj_controls;
+  /* precision record of the adjoint QP solve, optional: (batch) out, as in dmpc_group */
+  int32_t* num_pcg_corrections;
+  int32_t* num_pcg_fp64_iter;
 } dmpc_adjoint;
 
 /* Closed-loop rollout (benchmarking/reinforcement-learning/benchmark_diffmpc.py:140-175, the

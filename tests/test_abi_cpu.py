@@ -28,7 +28,7 @@ def test_library_loads_and_exports_every_header_symbol():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(_lib.EXPORTED_SYMBOLS)
-    assert lib.dmpc_abi_version() == _lib.ABI_VERSION == 2
+    assert lib.dmpc_abi_version() == _lib.ABI_VERSION == 3
 
 
 def test_defaults_match_reference_yaml():
