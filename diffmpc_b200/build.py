@@ -9,7 +9,8 @@ configuration (``-DDMPC_CFG=0``: up to 512 threads and one CTA per SM;
 256 threads and two CTAs per SM; ``3``: up to 384 threads, one CTA per SM, up to
 168 registers a thread), in parallel with the host side and the
 dense-layout kernels (``csrc/solver.cu``) and the XLA custom-call handler
-core (``csrc/xla_ffi.cc``); the objects are linked into one shared library.
+core (``csrc/xla_ffi.cc``; its XLA FFI symbols too when ``DMPC_XLA_INCLUDE`` names jaxlib's
+include directory); the objects are linked into one shared library.
 """
 
 import glob
@@ -30,8 +31,11 @@ UNITS = [
     ("k_sqp_cfg2.o", os.path.join(CSRC, "k_sqp.cu"), ["-DDMPC_CFG=2"]),
     ("k_sqp_cfg3.o", os.path.join(CSRC, "k_sqp.cu"), ["-DDMPC_CFG=3"]),
 ]
-if os.path.exists(os.path.join(CSRC, "xla_ffi.cc")):
-    UNITS.append(("xla_ffi.o", os.path.join(CSRC, "xla_ffi.cc"), []))
+# XLA custom-call handlers: the core always; the XLA FFI symbols when DMPC_XLA_INCLUDE names
+# jaxlib's include directory (the one holding xla/ffi/api/ffi.h)
+_XLA_INC = os.environ.get("DMPC_XLA_INCLUDE")
+UNITS.append(("xla_ffi.o", os.path.join(CSRC, "xla_ffi.cc"),
+              ["-DDMPC_WITH_XLA_FFI", "-I", _XLA_INC] if _XLA_INC else []))
 DEPS = glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

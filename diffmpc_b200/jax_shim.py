@@ -3,8 +3,11 @@
 ``make_jax_solve(solver)`` returns ``solve(x0, weights) -> (states, controls)``.
 - It is differentiable with ``jax.grad`` w.r.t. ``weights``, a dict of float64 arrays.
 - Its forward and backward run the CUDA kernels through ``jax.pure_callback``, handing the arrays over via host memory. This keeps existing JAX code (``jit``, ``grad``) working unchanged.
-- A zero-copy binding registers the C entry points as XLA FFI custom calls instead; the
-  handler that maps XLA buffers onto the C ABI is ``csrc/xla_ffi.cc``.
+- A zero-copy binding registers the C entry points as XLA FFI custom calls instead
+  (``register_ffi_targets``).  The handlers that map XLA buffers onto the C ABI are in
+  ``csrc/xla_ffi.cc`` (operand orders in ``include/dmpc_xla.h``); their core is built into
+  ``libdmpc.so`` and tested from C, the XLA-facing symbols only when the library is built with
+  ``DMPC_XLA_INCLUDE`` pointing at jaxlib's include directory.
 
 JAX and jaxlib are not installed in the image this library is built in, so this module is
 import-guarded and untested there.  ``make_jax_solve`` raises ImportError without jax.
@@ -18,6 +21,43 @@ try:  # pragma: no cover - exercised only where jax is installed
 except ImportError:  # pragma: no cover
     jax = None
     jnp = None
+
+
+FFI_TARGETS = (("dmpc_solve_fwd", "dmpc_xla_fwd_handler"), ("dmpc_solve_adj", "dmpc_xla_adj_handler"))
+
+
+def register_ffi_targets():
+    """Registers the library's XLA FFI handlers as the CUDA custom-call targets "dmpc_solve_fwd" and
+    "dmpc_solve_adj".  Needs jax and a ``libdmpc.so`` built with ``DMPC_XLA_INCLUDE`` (so that
+    ``csrc/xla_ffi.cc`` compiles its XLA part); unvalidated, since neither exists where this
+    library is built."""
+    if jax is None:
+        raise ImportError("diffmpc_b200.jax_shim needs jax and jaxlib (not installed)")
+    from diffmpc_b200 import _lib
+
+    lib = _lib.load()
+    for target, sym in FFI_TARGETS:
+        if not hasattr(lib, sym):
+            raise RuntimeError(f"{sym} is not in libdmpc.so: rebuild with DMPC_XLA_INCLUDE=<jaxlib>/include")
+        jax.ffi.register_ffi_target(target, jax.ffi.pycapsule(getattr(lib, sym)), platform="CUDA")
+
+
+def ffi_attributes(solver, batch: int):
+    """The custom calls' attributes for ``solver`` and a batch: the problem's integers and the
+    solver parameters as the raw bytes of a dmpc_solver_params."""
+    import numpy as np
+
+    from diffmpc_b200.sqp import solver_params_struct
+
+    prog = solver.program
+    dyn = prog.dynamics
+    return {
+        "model": dyn.model_id, "nx": prog.num_state_variables, "nu": prog.num_control_variables,
+        "horizon": prog.horizon, "batch": int(batch), "scheme": prog.discretization_scheme,
+        "penalize_control_reference": int(bool(prog.penalize_control_reference)),
+        "n_model_params": dyn.num_model_params(),
+        "solver_params": np.frombuffer(bytes(solver_params_struct(solver.params)), dtype=np.uint8),
+    }
 
 
 def make_jax_solve(solver, problem_params: Dict):

@@ -66,7 +66,7 @@ extern "C" {
 #define DMPC_STATUS_SUCCESS 0
 #define DMPC_STATUS_ERROR (-100)
 
-/* dynamics models (diffmpc/dynamics/*.py).  Model parameter vectors:
+/* dynamics models (diffmpc/dynamics/, one file per model).  Model parameter vectors:
  *   LINEAR      nx, nu free;  [A (nx*nx), B (nx*nu), b (nx)]     linear_dynamics.py:46-70
  *   QUADROTOR   nx=13, nu=4;  [mass, inertia (3x3 row-major, 9)] quadrotor_dynamics.py:84-133
  *   SPACECRAFT  nx=3,  nu=3;  [inertia_vector (3)]                spacecraft_dynamics.py:31-66
@@ -85,7 +85,7 @@ extern "C" {
 
 /* PCG arithmetic */
 #define DMPC_PREC_FP64 0   /* all-FP64 PCG, the reference's arithmetic */
-#define DMPC_PREC_MIXED 1  /* FP32 PCG iterations + FP64 iterative refinement */
+#define DMPC_PREC_MIXED 1  /* FP32 PCG iterations with FP64 residual replacement */
 
 #define DMPC_MAX_NX 32
 #define DMPC_MAX_NU 16
