@@ -262,7 +262,7 @@ def precision_record(solver, sol):
     out = {"qp_solves": int(ran.sum()), "replacements_per_qp": float(corr.mean()),
            "qp_handed_to_fp64": int((f64 > 0).sum()), "fp64_iter_share": float(f64.sum() / its.sum().clamp_min(1))}
     a, ai = solver.last_adjoint_pcg_record, solver.last_adjoint_pcg_iters
-    if a is not None and ai is not None:
+    if isinstance(a, torch.Tensor) and isinstance(ai, torch.Tensor):  # (per-group lists after solve_groups)
         out["adjoint"] = {"qp_solves": int(a.shape[1]), "replacements_per_qp": float(a[0].double().mean()),
                           "qp_handed_to_fp64": int((a[1] > 0).sum()),
                           "fp64_iter_share": float(a[1].double().sum() / ai.double().sum().clamp_min(1))}
@@ -678,21 +678,35 @@ def run_other_workload(args):
             groups.append((solver, p))
 
         def step():
-            probs = []
+            probs, ws = [], []
             for solver, p in groups:
-                w = {"initial_state": p["initial_state"].clone().requires_grad_(True)}
-                probs.append((solver, solver.initial_guess(p), p, w))
+                w = p["initial_state"].clone().requires_grad_(True)
+                ws.append(w)
+                probs.append((solver, solver.initial_guess(p), p, {"initial_state": w}))
             sols = solve_groups(probs)
-            sum((s.controls[:, 0] ** 2).sum() for s in sols).backward()
-            return sols
+            grads = torch.autograd.grad(sum((s.controls[:, 0] ** 2).sum() for s in sols), ws)
+            return sols, grads
 
-        ms, sols = _timed(step, args.steps, args.warmup)
+        from diffmpc_b200.autotune import tune_step
+        from diffmpc_b200.graph import CapturedStep
+
+        # launch shape: autotuned on this step (forward + adjoint, both groups), then the whole
+        # step (2 persistent launches and the loss) captured as one CUDA graph
+        ms_default, _ = _timed(step, 1, 1)
+        best = tune_step(groups[0][0], step, tag=f"mixed{B}", repeats=1, use_cache=False)
+        ms_eager, (sols, _) = _timed(step, args.steps, args.warmup)
+        cap = CapturedStep(step, warmup=args.warmup)
+        ms, (sols, _) = _timed(cap.replay, args.steps, args.warmup)
         iters = torch.cat([s.num_pcg_iters.sum(dim=1) for s in sols]).double().cpu()
-        line.update(metric="fwd+bwd MPC solves/s, 50% linear nx=12 / 50% quadrotor, N~U{20..100}, one launch each",
+        line.update(metric="fwd+bwd MPC solves/s, 50% linear nx=12 / 50% quadrotor, N~U{20..100}, "
+                           "one persistent launch per direction, CUDA graph, autotuned",
                     value=B / (ms * 1e-3), ms_per_step=ms, batch=B,
+                    eager_solves_per_s=B / (ms_eager * 1e-3), untuned_eager_solves_per_s=B / (ms_default * 1e-3),
+                    launch_shape={"cta_config": int(best[0]), "threads_per_block": int(best[1])},
                     pcg_iters_per_instance_p50=float(iters.quantile(0.5)),
                     pcg_iters_per_instance_p99=float(iters.quantile(0.99)),
-                    status_success=int(sum(int((s.status == 0).sum()) for s in sols)))
+                    status_success=int(sum(int((s.status == 0).sum()) for s in sols)),
+                    precision_record=[precision_record(s_, sol_) for (s_, _), sol_ in zip(groups, sols)])
     elif args.workload == "rollout":
         from diffmpc_b200.rollout import ClosedLoopRollout
 

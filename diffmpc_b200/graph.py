@@ -7,7 +7,10 @@ building descriptors and launching.  ``GraphedForward`` captures ONE
 initial state and warm start into those buffers and replays the graph: one graph
 launch, no host-side descriptor building.
 
-It is not differentiable.  Use ``SQPSolver.solve`` when gradients are needed.
+It is not differentiable.  ``CapturedStep`` captures a whole differentiable step instead:
+forward solves, the loss, and the adjoint launches of its backward pass (``solve_groups``
+over ragged groups, ``ClosedLoopRollout``, or plain ``SQPSolver.solve``), so that a training
+or evaluation loop on a fixed shape replays it as one graph.
 """
 
 from typing import Optional
@@ -75,3 +78,39 @@ class GraphedForward:
         c = self.call
         return SQPSolution(c.states, c.controls, c.dual, None, None, None, c.status, c.num_iter, c.conv,
                            c.conv_hist, c.alpha_hist, c.pcg_hist, None, c.lin_states, c.lin_controls)
+
+
+class CapturedStep:
+    """One CUDA graph of a whole step: ``fn()`` run once under capture, then ``replay()``.
+
+    ``fn`` takes no arguments.  It reads its inputs from tensors that outlive the capture (the
+    caller refills them in place between replays) and returns the tensors it produced (solution,
+    loss, gradients); it must not synchronise with the host (no ``.item()``, ``.cpu()`` or
+    printing of device values).  Take gradients with ``torch.autograd.grad`` rather than
+    ``backward()``: ``.grad`` accumulation would be captured as an accumulation.  ``warmup``
+    eager calls on a side stream come first: they set the kernels' launch attributes and
+    allocate the solver workspace and autograd buffers outside the capture.  ``replay()``
+    re-runs every captured launch (the solver kernels, their workspace resets and the loss's
+    torch kernels) and returns the tensors ``fn`` returned during capture, refreshed in place.
+    """
+
+    def __init__(self, fn, warmup: int = 3, device=None):
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.fn = fn
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            for _ in range(max(1, int(warmup))):
+                fn()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, capture_error_mode="relaxed"):
+            self.outputs = fn()
+
+    def replay(self):
+        self.graph.replay()
+        return self.outputs
+
+    __call__ = replay
+
