@@ -407,11 +407,16 @@ bool rows_path(const dmpc_solver_params* p, int nx, int K, int threads) {
 // the FP64 setup phases (assembly, factorisations) spread over all threads, and short horizons
 // leave too few rows to keep them busy (measured: nx=8, 40 knots runs 17 % faster at 256 threads
 // than at 160).
-int choose_threads_wide(const dmpc_solver_params* p, int nx, int K) {
+// One thread per PCG row (per knot and row quadruple on the row PCG), rounded up to whole warps,
+// at most 512.  The floor: 256 threads while the batch leaves SMs idle (fewer instances than
+// two per SM: the assembly and linearization phases then use the extra warps), 64 otherwise (small
+// instances then share an SM as several resident CTAs).
+int choose_threads_wide(const dmpc_solver_params* p, int nx, int K, bool busy) {
   int rows = K * nx;
   if (p->precision == DMPC_PREC_MIXED && rows_nx(nx) && K * ((nx + 3) / 4) <= 512) rows = K * ((nx + 3) / 4);
   int t = ((rows + 31) / 32) * 32;
-  if (t < 256) t = 256;
+  const int floor = busy ? 64 : 256;
+  if (t < floor) t = floor;
   if (t > 512) t = 512;
   return t;
 }
@@ -528,8 +533,9 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
   } else if (cfg == kCfgDual) {
     thr = 256;
   } else {
+    const bool busy = total >= 2 * dev.sms;
     for (int k = 0; k < n_groups; ++k) {
-      const int t = choose_threads_wide(p, groups[k].nx, groups[k].horizon + 1);
+      const int t = choose_threads_wide(p, groups[k].nx, groups[k].horizon + 1, busy);
       if (t > thr) thr = t;
     }
     if (thr > max_thr) thr = max_thr;

@@ -714,9 +714,10 @@ constexpr double kRestartRatio = 10.0;
 constexpr double kDivergeRatio = 1e4;
 // Stall detection: an FP32 segment (the iterations between two replacements) that runs past
 // max(kStallGrowth x the previous segment, kStallMin) iterations (kStallMin for the first) is cut
-// by a replacement, to which the stagnation rule then applies: an FP32 recursion that has
-// stopped falling on an ill-conditioned system goes to the FP64 recurrence after a few hundred
-// iterations instead of half the budget.
+// by a replacement, after which the FP32 PCG continues only if the true eta fell by the full
+// inner_rel_tol factor since the last replacement: an FP32 recursion that has stopped falling on
+// an ill-conditioned system, or falls far slower than before, goes to the FP64 recurrence after a
+// few hundred iterations instead of half the budget.
 constexpr int kStallMin = 200;
 constexpr int kStallGrowth = 4;
 __device__ __forceinline__ int next_stop(int it, int seg, int it_cap) {
@@ -978,7 +979,9 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
     // Residual replacement (see above); a non-finite segment is dropped.
     const bool bad = !(etap == etap) || !(vden == vden);
     const bool at_check = etap <= check_at;
-    const bool progressed = etap <= upd_rel * eta_upd || etap > hi || (it >= it_stop && it < it_cap);
+    const bool fell = etap <= upd_rel * eta_upd || etap > hi;
+    const bool cut = !fell && it >= it_stop && it < it_cap;  // ended by the stall detection
+    const bool progressed = fell || cut;
     for (int g = threadIdx.x; g < n; g += blockDim.x) {
       const int t = g / nx, x = t * ld + (g - t * nx);
       if (!bad) acc[g] += back * (double)dv[x];
@@ -1010,7 +1013,7 @@ __device__ __noinline__ PcgOut pcg_mixed_scaled(const Inst& s, double* lam, floa
     }
     const double etas = eta64 * s2;
     if (bad || nupd >= max_ref || it >= it_cap || !(etas > 0.0) ||
-        (progressed && !at_check && eta64 > kUpdateStagnation * prev64)) {
+        (progressed && !at_check && eta64 > (cut ? upd_rel : kUpdateStagnation) * prev64)) {
       if (!exact_now) flush();
       return fp64_finish(s, lam, it, max_iter, eps, red, par, nupd);
     }
@@ -1295,7 +1298,9 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
       const bool bad = !(etap == etap) || !(vden == vden);
       const bool at_check = etap <= check_at;
       // a segment cut by the stall detection counts as progress for the stagnation rule
-      const bool progressed = etap <= c_upd * eta_upd || (float)etap > hi || (it >= it_stop && it < it_cap);
+      const bool fell = etap <= c_upd * eta_upd || (float)etap > hi;
+      const bool cut = !fell && it >= it_stop && it < it_cap;  // ended by the stall detection
+      const bool progressed = fell || cut;
       // a non-finite segment is dropped: lam keeps the last finite update
       double a[R];
 #pragma unroll
@@ -1336,7 +1341,7 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
       }
       const double etas = eta64 * s2;
       if (bad || nupd >= c_maxref || it >= it_cap || !(etas > 0.0) ||
-          (progressed && !at_check && eta64 > kUpdateStagnation * prev64)) {
+          (progressed && !at_check && eta64 > (cut ? c_upd : kUpdateStagnation) * prev64)) {
         if (!exact) flush();
         return fp64_finish(s, lam, it, c_maxit, c_eps, red, par, nupd);
       }

@@ -59,7 +59,10 @@ class _RolloutFunction(torch.autograd.Function):
         f64 = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)  # noqa: E731
         i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
         linear = roll.simulator == "linear"
-        vec = lambda v, n: torch.as_tensor(v, dtype=torch.float64, device=dev).expand(n).contiguous()  # noqa: E731
+        # Python numbers are filled on the device: no host-to-device copy (CUDA-graph capture)
+        vec = lambda v, n: (torch.full((n,), float(v), dtype=torch.float64, device=dev)  # noqa: E731
+                            if isinstance(v, (int, float)) else
+                            torch.as_tensor(v, dtype=torch.float64, device=dev).expand(n).contiguous())
         cw = SimpleNamespace(ws=vec(roll.state_weight, nx), wc=vec(roll.control_weight, nu),
                              xr=None if roll.state_ref is None else vec(roll.state_ref, nx),
                              ur=None if roll.control_ref is None else vec(roll.control_ref, nu))

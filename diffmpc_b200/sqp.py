@@ -95,7 +95,11 @@ def _ptr(t):
 
 
 def _batched(v, base_shape, B, device, dtype=torch.float64):
-    """Broadcast a shared (base_shape) or per-instance (B, *base_shape) value to (B, *base)."""
+    """Broadcast a shared (base_shape) or per-instance (B, *base_shape) value to (B, *base).  A
+    Python number is filled on the device (no host-to-device copy, so that the call can be
+    captured in a CUDA graph)."""
+    if isinstance(v, (int, float)) and not isinstance(v, bool):
+        return torch.full((B, *base_shape), float(v), dtype=dtype, device=device)
     t = torch.as_tensor(v, dtype=dtype, device=device)
     n = 1
     for s in base_shape:

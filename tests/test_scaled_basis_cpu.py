@@ -108,15 +108,16 @@ STALL_MIN, STALL_GROWTH = 200, 4  # sqp_device.cuh: kStallMin, kStallGrowth
 
 
 def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_iter=10000, Pd=None, max_ref=30,
-                     stall=True, stats=None):
+                     stall=True, stats=None, stall_min=STALL_MIN, stall_growth=STALL_GROWTH):
     """Numpy restatement of the kernels' mixed recurrence (sqp_device.cuh: pcg_rows_scaled,
     pcg_mixed_scaled): FP32 vectors and FP32 F^, FP64 dot products, and the FP32 residual replaced
     by the FP64 one, r^ = r^_0 + (I + F^) lam^, each time the recursion's eta falls by `upd_rel`;
     convergence is decided on an exact residual gamma - S lam.  With `stall`, an FP32 segment is
-    also cut after max(4 x the previous segment, 200) iterations (200 for the first).  With Pd
-    given, the kernels' hand-over rules apply (a replacement triggered by the recursion's fall, by
-    its divergence or by the stall cut whose true eta fell by less than 100x; half the budget or
-    max_ref replacements spent) and the FP64 recurrence finishes; the replacement count is then
+    also cut after max(stall_growth x the previous segment, stall_min) iterations (stall_min for
+    the first; the kernels' 4 and 200 by default).  With Pd
+    given, the kernels' hand-over rules apply (a replacement triggered by the recursion's fall or
+    its divergence whose true eta fell by less than 100x, or by the stall cut whose true eta fell
+    by less than 1/upd_rel; half the budget or max_ref replacements spent) and the FP64 recurrence finishes; the replacement count is then
     returned negated and, with `stats` (a dict), the FP64 iteration count stored under "fp64".
     Returns (lam, iterations, replacements, eta64)."""
     f32, f64 = np.float32, np.float64
@@ -138,7 +139,7 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
     eta_upd, prev64 = eta, eta64
     it = nrep = seg0 = 0
     it_cap = max_iter // 2
-    it_stop = min(it_cap, STALL_MIN) if stall else it_cap
+    it_stop = min(it_cap, stall_min) if stall else it_cap
     while True:
         u = -(p + F32 @ p)
         vden = float(p.astype(f64) @ u.astype(f64))
@@ -155,7 +156,9 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
         acc = acc + d.astype(f64) / scale
         d = np.zeros_like(r)
         at_check = etap <= check_at
-        progressed = etap <= upd_rel * eta_upd or etap > hi or it_stop <= it < it_cap
+        fell = etap <= upd_rel * eta_upd or etap > hi
+        cut = not fell and it_stop <= it < it_cap  # ended by the stall detection
+        progressed = fell or cut
         exact = at_check
         if not exact:
             rh = rh0 + acc + F64 @ acc
@@ -171,7 +174,7 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
         if not abs(eta64) > eps:
             return lam + Li.T @ acc, it, nrep, eta64
         etas = eta64 * s2
-        stalled = progressed and not at_check and eta64 > 1e-2 * prev64
+        stalled = progressed and not at_check and eta64 > (upd_rel if cut else 1e-2) * prev64
         if Pd is not None and (it >= it_cap or nrep >= max_ref or stalled):
             lam, it64, e = _fp64_finish(Sd, Pd, gam, lam + Li.T @ acc, eps, max_iter)
             if stats is not None:
@@ -180,7 +183,7 @@ def _pcg_replacement(Fh, Li, Sd, gam, eps, upd_rel=1e-3, check_margin=0.1, max_i
         assert it < it_cap, "FP32 share of the budget exhausted"
         eta_upd, prev64 = etas, eta64
         if stall:
-            it_stop = min(it_cap, it + max(STALL_GROWTH * (it - seg0), STALL_MIN))
+            it_stop = min(it_cap, it + max(stall_growth * (it - seg0), stall_min))
         seg0 = it
         r = (scale * rh).astype(f32)
         z = (scale * (rh - F64 @ rh)).astype(f32)
@@ -312,3 +315,37 @@ def test_ill_conditioned_systems_hand_over_to_fp64_and_match_the_reference_recur
         st_off = {}
         _, it_off, nrep_off, _ = _pcg_replacement(Fh, Li, Sd, g, eps, Pd=Pd, stall=False, stats=st_off)
         assert nrep_off < 0 and it_off - st_off["fp64"] >= 3000, (seed, it_off, st_off)
+
+
+def test_stall_thresholds_leave_the_headline_qps_in_fp32():
+    """The stall cut's thresholds against the QPs of the headline workload (quadrotor N=60, the
+    first SQP iteration of four instances, the oracle's S and Phi^-1, eps 1e-20 relative): at the
+    kernels' max(4 x previous, 200) no QP is handed to the FP64 recurrence; a tighter
+    max(2 x previous, 50) hands some over although FP32 finishes them in fewer iteration-costs."""
+    from diffmpc_b200 import workloads
+    from tests.oracle_util import oracle_solver, tensor_params
+
+    dyn, st, bt, sp = workloads.quadrotor(B=4, N=60, seed=1002)
+    os_ = oracle_solver(dyn, st, sp)
+    tp = tensor_params(bt)
+    g0 = os_.initial_guess(tp)
+    _, _, schur = os_.compute_qp_parameters(g0.states, g0.controls, tp)
+    tight_handovers = 0
+    for i in range(4):
+        S, Phi = schur.S[i:i + 1], schur.preconditioner_Phiinv[i:i + 1]
+        K, nx = S.shape[1], S.shape[2]
+        Sd, Pd = _dense(S, K, nx).numpy(), _dense(Phi, K, nx).numpy()
+        n = K * nx
+        L = np.zeros((n, n))
+        for t in range(K):
+            L[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx] = np.linalg.cholesky(-Sd[t * nx:(t + 1) * nx, t * nx:(t + 1) * nx])
+        Li = np.linalg.inv(L)
+        Fh = -(Li @ Sd @ Li.T) - np.eye(n)
+        g = np.random.default_rng(i).standard_normal(n)
+        eps = 1e-20 * float(g @ g)
+        _, _, nrep, eta = _pcg_replacement(Fh, Li, Sd, g, eps, Pd=Pd)
+        assert nrep > 0 and abs(eta) <= eps, (i, nrep)
+        _, _, nrep_t, _ = _pcg_replacement(Fh, Li, Sd, g, eps, Pd=Pd, stall_min=50, stall_growth=2)
+        tight_handovers += nrep_t < 0
+    assert tight_handovers >= 1
+
