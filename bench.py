@@ -39,6 +39,9 @@ GRAD_KEYS = ("initial_state", "weights_penalization_reference_state_trajectory",
              "weights_penalization_control_squared", "mass")
 
 
+CTA_CONFIGS = {"auto": 0, "wide": 1, "rows": 2, "dual": 3}  # DMPC_CTA_*
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -54,6 +57,10 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
+    ap.add_argument("--cta-config", default="auto", choices=["auto", "wide", "rows", "dual"],
+                    help="CTA shape of the solver kernels (dmpc_solver_params.cta_config)")
+    ap.add_argument("--blocks-in-smem", type=int, default=-1, choices=[-1, 0, 1],
+                    help="dmpc_solver_params.blocks_in_smem (-1: shared memory when they fit)")
     ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress", "rollout", "rollout_spacecraft"],
                     help="quadrotor = the headline; the others report the remaining workload shapes")
     return ap.parse_args()
@@ -152,6 +159,8 @@ def build(args, rank):
     dyn, st, bt, sp = workloads.quadrotor(B=args.batch, N=args.horizon, seed=1002 + rank)
     sp["precision"] = args.precision
     sp["pcg"]["tol_epsilon"] = args.pcg_tol
+    sp["cta_config"] = CTA_CONFIGS[args.cta_config]
+    sp["blocks_in_smem"] = args.blocks_in_smem
     return dyn, st, bt, sp
 
 

@@ -107,24 +107,38 @@ __host__ __device__ inline Layout make_layout(int nx, int nu, int N, int ld32, b
 // distinct banks, and ld is even, so every row starts 8-byte aligned.
 __host__ __device__ constexpr int pad_ld(int nx) { return nx + ((6 - nx % 4) % 4); }
 
-// shared memory bytes of one CTA: 2x64 reduction doubles + 8 line-search values + PCG vectors
-// (+ FP32 blocks)
-__host__ __device__ inline size_t smem_bytes_for(int nx, int N, int precision, bool blocks_smem) {
-  const size_t K = N + 1;
-  size_t b = 136 * sizeof(double);
-  if (precision == DMPC_PREC_FP64) {
-    b += 5 * K * nx * sizeof(double);
-  } else {
-    b += align_up(5 * (K + 2) * pad_ld(nx) * sizeof(float), 16);
-    if (blocks_smem) b += (size_t)K * nx * pad_ld(nx) * sizeof(float);
-  }
-  return align_up(b, 16);
-}
-
 // nx with a compile-time row PCG (pcg_rows_scaled, 4 rows per thread, ceil(nx / 4) threads per
-// knot)
+// knot; pcg_rows_t in the two-CTA configuration, rows_tpk(nx) threads per knot)
 __host__ __device__ inline bool rows_nx(int nx) {
   return nx == 3 || nx == 4 || nx == 6 || nx == 7 || nx == 8 || nx == 12 || nx == 13;
+}
+
+// Threads per knot of the two-CTA row PCG (pcg_rows_t): 4 rows each, a power of two.
+__host__ __device__ constexpr int rows_tpk(int nx) { return nx <= 4 ? 1 : (nx <= 8 ? 2 : 4); }
+
+// Bytes of the PCG vectors in shared memory (16-byte multiple).  FP64: five K nx vectors.
+// Mixed: five padded FP32 vectors of K + 2 segments (the generic PCG; the row PCG uses two and
+// keeps its FP64 exchange vector in the rest); in the two-CTA configuration with a row PCG, the
+// larger of that and pcg_rows_t's four FP32 vectors of K + 2 segments of 4 rows_tpk(nx) floats
+// plus its FP64 exchange vector (K + 2 segments of nx) and 12 constants.
+__host__ __device__ inline size_t pcg_vec_bytes(int nx, int K, int precision, int cfg) {
+  if (precision == DMPC_PREC_FP64) return 5 * (size_t)K * nx * sizeof(double);
+  size_t b = align_up(5 * (size_t)(K + 2) * pad_ld(nx) * sizeof(float), 16);
+  if (cfg == kCfgDual && rows_nx(nx)) {
+    const size_t t = 4 * (size_t)(K + 2) * 4 * rows_tpk(nx) * sizeof(float) +
+                     ((size_t)(K + 2) * nx + 12) * sizeof(double);
+    if (align_up(t, 16) > b) b = align_up(t, 16);
+  }
+  return b;
+}
+
+// shared memory bytes of one CTA: 2x64 reduction doubles + 8 line-search values + PCG vectors
+// (+ FP32 blocks)
+__host__ __device__ inline size_t smem_bytes_for(int nx, int N, int precision, bool blocks_smem, int cfg) {
+  const size_t K = N + 1;
+  size_t b = 136 * sizeof(double) + pcg_vec_bytes(nx, (int)K, precision, cfg);
+  if (precision != DMPC_PREC_FP64 && blocks_smem) b += (size_t)K * nx * pad_ld(nx) * sizeof(float);
+  return align_up(b, 16);
 }
 
 // What each kernel launch does.

@@ -398,8 +398,9 @@ DeviceInfo device_info() {
 
 // Mixed precision takes the compile-time row PCG (pcg_rows_scaled, 4 rows per thread) when the
 // instance's K ceil(nx / 4) threads fit the CTA.
-bool rows_path(const dmpc_solver_params* p, int nx, int K, int threads) {
-  return p->precision == DMPC_PREC_MIXED && rows_nx(nx) && K * ((nx + 3) / 4) <= threads;
+bool rows_path(const dmpc_solver_params* p, int nx, int K, int threads, int cfg = kCfgRows) {
+  const int tpk = cfg == kCfgDual ? rows_tpk(nx) : (nx + 3) / 4;
+  return p->precision == DMPC_PREC_MIXED && rows_nx(nx) && K * tpk <= threads;
 }
 
 // Threads per CTA (256..512): one thread per knot and row quadruple of the row PCG when it
@@ -424,19 +425,21 @@ int choose_threads_wide(const dmpc_solver_params* p, int nx, int K, bool busy) {
 // Shared memory one CTA needs for a group, and where the group's blocks go (G.blocks_smem,
 // G.w64_off, G.smem_block_budget), for a CTA of `threads` threads with at most `cap` bytes.
 // Returns 0 when even the minimum does not fit.
-size_t group_smem(const dmpc_solver_params* p, const dmpc_group& g, DevGroup& G, int threads, size_t cap) {
-  const size_t base = smem_bytes_for(g.nx, g.horizon, p->precision, false);
+size_t group_smem(const dmpc_solver_params* p, const dmpc_group& g, DevGroup& G, int threads, size_t cap, int cfg) {
+  const size_t base = smem_bytes_for(g.nx, g.horizon, p->precision, false, cfg);
   G.blocks_smem = 0;
   G.smem_block_budget = 0;
   G.w64_off = 0;
   if (base > cap) return 0;
   if (p->precision != DMPC_PREC_MIXED) return base;
-  if (rows_path(p, g.nx, G.K, threads) && p->blocks_in_smem != 1) {
+  if (rows_path(p, g.nx, G.K, threads, cfg) && p->blocks_in_smem != 1) {
     // The row PCG reads the FP32 W blocks once per FP32 segment into registers (they stay in
     // the workspace); the FP64 W blocks of its residual replacements go to shared memory if they
-    // fit.
+    // fit, except in the two-CTA configuration: there they would take most of the SM's shared
+    // memory from L1, and the replacements are rare (measured: the quadrotor N=60 headline runs
+    // 7 % faster with them in the workspace).
     const size_t w64b = (size_t)G.K * g.nx * g.nx * sizeof(double);
-    if (p->blocks_in_smem != 0 && align_up(base, 16) + w64b <= cap) {
+    if (p->blocks_in_smem != 0 && cfg != kCfgDual && align_up(base, 16) + w64b <= cap) {
       G.w64_off = (uint32_t)align_up(base, 16);
       return G.w64_off + w64b;
     }
@@ -445,7 +448,7 @@ size_t group_smem(const dmpc_solver_params* p, const dmpc_group& g, DevGroup& G,
   // Generic path: FP32 blocks for every instance in shared memory (1); in a ragged group whose
   // longest instance does not fit, each instance checks its own size at run time (2); else
   // workspace (0).  Per-instance horizons live in device memory, hence mode 2.
-  const size_t need_all = smem_bytes_for(g.nx, g.horizon, p->precision, true);
+  const size_t need_all = smem_bytes_for(g.nx, g.horizon, p->precision, true, cfg);
   if (p->blocks_in_smem != 0) {
     if (need_all <= cap) {
       G.blocks_smem = 1;
@@ -510,18 +513,27 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     }
     total += g.batch;
   }
-  // configuration: the row configuration when every group is mixed precision with a
-  // compile-time row PCG whose K ceil(nx/4) threads fit 384, or ragged (instances too long for
-  // it take the generic PCG inside the same launch), unless the caller chose another
+  // configuration, unless the caller chose one:
+  // - two CTAs per SM (pcg_rows_t) when every group is mixed precision with a compile-time row
+  //   layout whose K rows_tpk(nx) threads fit 256, the one-CTA row layout would need more than
+  //   128 threads (so that it would hold one instance per SM), and the batch has more instances
+  //   than SMs (measured: quadrotor N=60, B=4096, 22 % faster than the one-CTA row layout);
+  // - else the row configuration when every group has a compile-time row PCG whose K ceil(nx/4)
+  //   threads fit 384, or is ragged (instances too long for it take the generic PCG inside the
+  //   same launch);
+  // - else the wide configuration.
   int cfg = kCfgWide;
   if (p->cta_config == DMPC_CTA_ROWS) cfg = kCfgRows;
   else if (p->cta_config == DMPC_CTA_DUAL) cfg = kCfgDual;
   else if (p->cta_config == DMPC_CTA_AUTO && (p->threads_per_block == 0 || p->threads_per_block <= 384)) {
-    bool rows = true;
-    for (int k = 0; rows && k < n_groups; ++k)
-      rows = rows_path(p, groups[k].nx, groups[k].horizon + 1, 384) ||
-             (p->precision == DMPC_PREC_MIXED && rows_nx(groups[k].nx) && groups[k].horizons);
-    if (rows) cfg = kCfgRows;
+    bool rows = true, dual = p->threads_per_block == 0 || p->threads_per_block == 256;
+    for (int k = 0; k < n_groups; ++k) {
+      const int nx = groups[k].nx, K = groups[k].horizon + 1;
+      rows = rows && (rows_path(p, nx, K, 384) || (p->precision == DMPC_PREC_MIXED && rows_nx(nx) && groups[k].horizons));
+      dual = dual && rows_path(p, nx, K, 256, kCfgDual) && K * ((nx + 3) / 4) > 128;
+    }
+    if (dual && total > dev.sms) cfg = kCfgDual;
+    else if (rows) cfg = kCfgRows;
   }
   const int max_thr = cfg == kCfgWide ? 512 : (cfg == kCfgRows ? 384 : 256);
   if (p->threads_per_block > max_thr || (cfg == kCfgDual && p->threads_per_block != 0 && p->threads_per_block != 256))
@@ -548,7 +560,7 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
   for (int k = 0; k < n_groups; ++k) {
     const dmpc_group& g = groups[k];
     DevGroup& G = args->grp[k];
-    const size_t sm = group_smem(p, g, G, thr, cap);
+    const size_t sm = group_smem(p, g, G, thr, cap, cfg);
     if (sm == 0) return DMPC_ERR_UNSUPPORTED;
     if (sm > smax) smax = sm;
     const int ng = adj ? adj[k].n_param_grads : g.n_model_params;  // size for any later adjoint call

@@ -719,7 +719,7 @@ constexpr double kDivergeRatio = 1e4;
 // an ill-conditioned system, or falls far slower than before, goes to the FP64 recurrence after a
 // few hundred iterations instead of half the budget.
 constexpr int kStallMin = 200;
-constexpr int kStallGrowth = 4;
+constexpr int kStallGrowth = 2;
 __device__ __forceinline__ int next_stop(int it, int seg, int it_cap) {
   return min(it_cap, it + max(kStallGrowth * seg, kStallMin));
 }
@@ -751,30 +751,33 @@ __device__ __forceinline__ T* as_shared(T* p) {
   return reinterpret_cast<T*>(g_dyn_smem + off);
 }
 
-// Compile-time-nx FP64 helpers of the row PCG (pcg_rows_scaled): rows q + k TPK (k < R,
-// TPK = ceil(NX / R)) of knot t; a row past NX, or a thread without a knot (ok false), is
-// skipped.  They stay out of line, so that their registers do not weigh on the allocation of the
-// FP32 iteration loop that calls them on its cold path.
+// Compile-time-nx FP64 helpers of the row PCGs: rows q + k TPK (k < R, TPK = ceil(NX / R)) of
+// knot t for pcg_rows_scaled, rows R q + k for pcg_rows_t (CONTIG); a row past NX, or a thread
+// without a knot (ok false), is skipped.  They stay out of line, so that their registers do not
+// weigh on the allocation of the FP32 iteration loop that calls them on its cold path.
 template <int NX, int R>
 struct RowVals {
   double v[R];
 };
+template <int NX, int R, bool CONTIG>
+__device__ __forceinline__ int row_of(int q, int k) {
+  return CONTIG ? R * q + k : q + k * ((NX + R - 1) / R);
+}
 
 // res = gamma - S lam for the thread's rows and r^ = L^-1 res in t1 (one barrier between the
 // passes; each thread reads back only its own t1 rows).
-template <int NX, int R>
+template <int NX, int R, bool CONTIG = false>
 __device__ __noinline__ void exact_rhat_rows(const Inst& s, const double* lam, int t, int q, bool ok, int N) {
-  constexpr int TPK = (NX + R - 1) / R;
 #pragma unroll
   for (int k = 0; k < R; ++k) {
-    const int i = q + k * TPK;
+    const int i = row_of<NX, R, CONTIG>(q, k);
     if (ok && i < NX) s.res[t * NX + i] = s.gam[t * NX + i] + stencil64<NX>(s.th, s.ph, lam, t, i, N);
   }
   __syncthreads();
   const double* x = s.res + t * NX;
 #pragma unroll
   for (int k = 0; k < R; ++k) {
-    const int i = q + k * TPK;
+    const int i = row_of<NX, R, CONTIG>(q, k);
     if (ok && i < NX) {
       const double* m = s.li + (size_t)(t * NX + i) * NX;
       double a = 0.0;
@@ -789,10 +792,10 @@ __device__ __noinline__ void exact_rhat_rows(const Inst& s, const double* lam, i
 // (F^ v) for the thread's rows in FP64: W_t (block t-1 of w, row stride NX) times v_{t-1} plus
 // W_{t+1}^T (block t) times v_{t+1}; block N is zero and stands in for W_0 and W_{N+1}.  v points
 // at knot 0 of a vector with zero segments at knots -1 and K.  A row past NX repeats row q.
-template <int NX, int R>
+template <int NX, int R, bool CONTIG = false>
 __device__ __noinline__ RowVals<NX, R> fhat64_rows(const double* __restrict__ w, int N, int t, int q,
                                                    const double* v) {
-  constexpr int BS = NX * NX, TPK = (NX + R - 1) / R;
+  constexpr int BS = NX * NX;
   const double* lo = w + (size_t)(t > 0 ? t - 1 : N) * BS;
   const double* up = w + (size_t)(t < N ? t : N) * BS;
   const double* vm = v + (t - 1) * NX;
@@ -803,7 +806,7 @@ __device__ __noinline__ RowVals<NX, R> fhat64_rows(const double* __restrict__ w,
   for (int k = 0; k < R; ++k) {
     a[k] = 0.0;
     b[k] = 0.0;
-    ii[k] = (q + k * TPK < NX) ? q + k * TPK : q;
+    ii[k] = (row_of<NX, R, CONTIG>(q, k) < NX) ? row_of<NX, R, CONTIG>(q, k) : q;
   }
 #pragma unroll
   for (int j = 0; j < NX; ++j) {
@@ -1377,6 +1380,343 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
   return PcgOut{it, eta64, nrep_out};
 }
 
+// Two CTAs per SM (kCfgDual: 256 threads, 128 registers a thread).  Compile-time nx, TPK threads
+// per knot (TPK = 1, 2, 4 for nx <= 4, 8, 16), K TPK <= blockDim.  Thread (t, q) = (tid div TPK,
+// tid mod TPK) owns rows 4q .. 4q + 3 of block row t and keeps those rows of W_t, padded to
+// PD = 4 TPK columns, in registers: 4 PD floats (64 for the quadrotor), ONE copy of each W block
+// instead of the row layout's two (W_t rows and W_{t+1} columns), which is what lets two
+// instances share an SM.  Both products of F^ v come from those registers:
+//   lower  (W_t v_{t-1})_i      = sum_j W_t[i, j] v_{t-1, j}: the thread's rows, v_{t-1} from
+//                                 shared memory;
+//   upper  (W_t^T v_t)_j        = sum_i W_t[i, j] v_{t, i}: the thread's share from its own v_t
+//                                 rows (registers), summed over the knot's TPK lanes by a
+//                                 reduce-scatter of warp shuffles (log2 TPK rounds), after
+//                                 which lane q holds columns 4q .. 4q + 3.  They are knot t-1's
+//                                 upper term and go to shared memory (segment t-1 of `up`) in
+//                                 the same barrier interval as v_t itself.
+// So that the reduce-scatter needs no selects, lane q keeps its W columns in an order that puts
+// the columns it sends in the first half of its registers at each round: register group g holds
+// column group g ^ (TPK - 1 - q).  The lower product reads v_{t-1} in that order (float4 loads).
+// Threads past the last knot idle on knot 0 with zero coefficients, store nothing and add zeros
+// to the reductions.  Everything else (scaling, FP64 residual replacement, stall detection,
+// hand-over to the FP64 recurrence, stopping test) follows pcg_rows_scaled line by line.
+template <int NX, int TPK>
+__device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec, int max_iter, double eps,
+                                          int max_ref, double upd_rel, double* red, int& par_io) {
+  int par = par_io;  // the reduction parity in a register; written back on every return
+  constexpr int R = 4;
+  constexpr int PD = R * TPK;  // padded rows / columns of a knot, the segment stride of the vectors
+  constexpr int LD = pad_ld(NX);
+  constexpr int BS = NX * LD;
+  static_assert(NX <= PD && (TPK == 1 || TPK == 2 || TPK == 4), "row layout");
+  const int K = s.K, N = s.N;
+  const int span = (K + 2) * PD;
+  float* rbase = as_shared(vec);  // four vectors of K + 2 segments: knots -1 .. K
+  float* rv = rbase + PD;
+  float* pv = rv + span;
+  float* upr = pv + span;  // upr / upp segment t: (W_{t+1}^T v_{t+1}) for knot t's rows
+  float* upp = upr + span;
+  red = as_shared(red);
+  const int lane_q = threadIdx.x % TPK;
+  const bool ok = (int)threadIdx.x < TPK * K;
+  const int q = ok ? lane_q : 0;
+  const int tc = ok ? (int)threadIdx.x / TPK : 0;
+  auto row = [&](int k) { return R * q + k; };
+  auto has = [&](int k) { return ok && R * q + k < NX; };
+  auto cgrp = [&](int g) { return g ^ (TPK - 1 - lane_q); };  // column group of register group g
+  for (int w = threadIdx.x; w < 4 * span; w += blockDim.x) rbase[w] = 0.f;
+  // v_t rows (own) -> v store and the upper term for knot t-1 (before the barrier)
+  auto push = [&](const float (&w)[R][PD], const float* x, float* v, float* up) {
+    float c[PD];
+#pragma unroll
+    for (int m = 0; m < PD; ++m) c[m] = 0.f;
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+#pragma unroll
+      for (int m = 0; m < PD; ++m) c[m] = fmaf(w[k][m], x[k], c[m]);
+    float y[R];
+    if constexpr (TPK == 4) {
+      float h[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) h[j] = c[8 + j] + __shfl_xor_sync(DMPC_FULL_MASK, c[j], 2);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) y[j] = h[4 + j] + __shfl_xor_sync(DMPC_FULL_MASK, h[j], 1);
+    } else if constexpr (TPK == 2) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) y[j] = c[4 + j] + __shfl_xor_sync(DMPC_FULL_MASK, c[j], 1);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) y[j] = c[j];
+    }
+    if (ok) {
+      *reinterpret_cast<float4*>(v + tc * PD + R * q) = make_float4(x[0], x[1], x[2], x[3]);
+      *reinterpret_cast<float4*>(up + (tc - 1) * PD + R * q) = make_float4(y[0], y[1], y[2], y[3]);
+    }
+  };
+  // (F^ v) for the thread's rows after the barrier: lower term from v_{t-1}, upper from `up`
+  auto pull = [&](const float (&w)[R][PD], const float* v, const float* up, float* f) {
+    float a[R], b[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      a[k] = 0.f;
+      b[k] = 0.f;
+    }
+    const float* vm = v + (tc - 1) * PD;
+#pragma unroll
+    for (int g = 0; g < TPK; ++g) {
+      const float4 y = *reinterpret_cast<const float4*>(vm + 4 * cgrp(g));
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        a[k] = fmaf(w[k][4 * g], y.x, a[k]);
+        b[k] = fmaf(w[k][4 * g + 1], y.y, b[k]);
+        a[k] = fmaf(w[k][4 * g + 2], y.z, a[k]);
+        b[k] = fmaf(w[k][4 * g + 3], y.w, b[k]);
+      }
+    }
+    const float4 u = *reinterpret_cast<const float4*>(up + tc * PD + R * q);
+    f[0] = ok ? a[0] + b[0] + u.x : 0.f;
+    f[1] = ok ? a[1] + b[1] + u.y : 0.f;
+    f[2] = ok ? a[2] + b[2] + u.z : 0.f;
+    f[3] = ok ? a[3] + b[3] + u.w : 0.f;
+  };
+  auto dot32 = [&](const float* a, const float* b) {
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      if (has(k)) acc = fmaf(a[k], b[k], acc);
+    return acc;
+  };
+  const int w2 = warp_pow2();
+  // FP64 exchange vector (knots -1..K) after the four FP32 vectors, then the solve's constants
+  auto x64_of = [&]() { return reinterpret_cast<double*>(as_shared(vec + 4 * span)) + NX; };
+  {
+    double* x64 = x64_of();
+    for (int w = threadIdx.x; w < NX; w += blockDim.x) {
+      x64[w - NX] = 0.0;
+      x64[K * NX + w] = 0.0;
+    }
+  }
+  auto eta_of = [&](const double* rh, double* zh) -> double {
+    double* x64 = x64_of();
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      if (has(k)) x64[tc * NX + row(k)] = rh[k];
+    __syncthreads();
+    const RowVals<NX, R> h = fhat64_rows<NX, R, true>(s.pm, N, tc, q, x64);
+    double e = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      zh[k] = rh[k] - h.v[k];
+      if (has(k)) e += rh[k] * zh[k];
+    }
+    return e;
+  };
+  auto flush = [&]() {
+    double* acc = s.tmp;
+    __syncthreads();
+    double l[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) l[k] = lower_col_t<NX>(s.li, tc, has(k) ? row(k) : q, acc + tc * NX);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      if (has(k)) {
+        lam[tc * NX + row(k)] += l[k];
+        acc[tc * NX + row(k)] = 0.0;
+      }
+    __syncthreads();
+  };
+  // W_t rows 4q..4q+3 in register-group order (block t-1 of w32; block N is zero and stands in
+  // for W_0); zero past NX and on idle threads
+  auto load_w = [&](float (&w)[R][PD]) {
+    const float* wb = s.w32 + (tc > 0 ? tc - 1 : N) * BS;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int i = R * q + k;
+#pragma unroll
+      for (int g = 0; g < TPK; ++g)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const int c = 4 * cgrp(g) + kk;
+          w[k][4 * g + kk] = (ok && i < NX && c < NX) ? wb[i * LD + c] : 0.f;
+        }
+    }
+  };
+  float r[R], p[R], d[R], f[R];
+  int it = 0;
+  double eta;
+  float trig, hi;
+  {
+    double rh[R], zh[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      d[k] = 0.f;
+      if (has(k)) s.tmp[tc * NX + row(k)] = 0.0;
+    }
+    exact_rhat_rows<NX, R, true>(s, lam, tc, q, ok, N);
+#pragma unroll
+    for (int k = 0; k < R; ++k) rh[k] = has(k) ? s.t1[tc * NX + row(k)] : 0.0;
+    const double eta64 = block_sum2(eta_of(rh, zh), red, par);
+    if (!(eta64 == eta64)) {
+      par_io = par;
+      return PcgOut{it, eta64};
+    }
+    const double scale = (eta64 > 0.0) ? rsqrt(eta64) : 1.0;
+    double* cst = x64_of() + (K + 1) * NX;
+    if (threadIdx.x == 0) {
+      cst[0] = scale;
+      cst[1] = (eta64 > 0.0) ? sqrt(eta64) : 1.0;
+      cst[2] = scale * scale;
+      cst[3] = eps * scale * scale * kCheckMargin;
+      cst[4] = eta64;
+      cst[5] = eta64 * scale * scale;
+      cst[6] = eps;
+      cst[7] = upd_rel;
+      cst[8] = (double)max_ref;
+      cst[9] = 0.0;
+      cst[10] = (double)max_iter;
+      cst[11] = 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      r[k] = has(k) ? (float)(scale * rh[k]) : 0.f;
+      p[k] = has(k) ? (float)(scale * zh[k]) : 0.f;
+    }
+    eta = eta64 * scale * scale;
+    trig = (float)fmax(eps * scale * scale * kCheckMargin, upd_rel * eta);
+    hi = (float)(kDivergeRatio * eta);
+  }
+  int it_stop = min(max_iter / 2, kStallMin);
+  int nrep_out;
+  double eta64 = 0.0;
+  for (;;) {
+    double vden, etap;
+    float z[R];
+    {
+      float w[R][PD];
+      load_w(w);
+      // p^ and its upper term: the first segment's, or p after a replacement
+      __syncthreads();
+      push(w, p, pv, upp);
+      __syncthreads();
+      for (;;) {
+        // u^ = S^ p^ = -(p^ + F^ p^)
+        float u[R];
+        pull(w, pv, upp, f);
+#pragma unroll
+        for (int k = 0; k < R; ++k) u[k] = -(p[k] + f[k]);
+        vden = block_sum_f32w(dot32(p, u), red, par, w2);
+        const float alpha = quot32(eta, vden);
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          d[k] = fmaf(alpha, p[k], d[k]);
+          r[k] = fmaf(-alpha, u[k], r[k]);
+        }
+        push(w, r, rv, upr);
+        __syncthreads();
+        // z^ = Phi^ r^ = r^ - F^ r^
+        pull(w, rv, upr, f);
+#pragma unroll
+        for (int k = 0; k < R; ++k) z[k] = r[k] - f[k];
+        etap = block_sum_f32w(dot32(r, z), red, par, w2);
+        ++it;
+        const float etaf = (float)etap;
+        if (!(etaf > trig) || etaf > hi || it >= it_stop || !(vden == vden)) break;
+        const float beta = quot32(etap, eta);
+#pragma unroll
+        for (int k = 0; k < R; ++k) p[k] = fmaf(beta, p[k], z[k]);
+        push(w, p, pv, upp);
+        eta = etap;
+        __syncthreads();
+      }
+    }
+    {
+      // Residual replacement, as in pcg_rows_scaled.
+      double* cst = x64_of() + (K + 1) * NX;
+      double* acc = s.tmp;
+      const double scale = cst[0], back = cst[1], s2 = cst[2], check_at = cst[3], prev64 = cst[4],
+                   eta_upd = cst[5], c_eps = cst[6], c_upd = cst[7];
+      const int c_maxref = (int)cst[8], nupd = (int)cst[9] + 1, c_maxit = (int)cst[10], it_cap = c_maxit / 2;
+      const bool bad = !(etap == etap) || !(vden == vden);
+      const bool at_check = etap <= check_at;
+      const bool fell = etap <= c_upd * eta_upd || (float)etap > hi;
+      const bool cut = !fell && it >= it_stop && it < it_cap;
+      const bool progressed = fell || cut;
+      double a[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        a[k] = has(k) ? acc[tc * NX + row(k)] : 0.0;
+        if (!bad) {
+          a[k] += back * (double)d[k];
+          if (has(k)) acc[tc * NX + row(k)] = a[k];
+        }
+        d[k] = 0.f;
+      }
+      double rh[R], zh[R];
+      bool exact = bad || at_check || it >= it_cap;
+      if (!exact) {
+        double* x64 = x64_of();
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+          if (has(k)) x64[tc * NX + row(k)] = a[k];
+        __syncthreads();
+        const RowVals<NX, R> h = fhat64_rows<NX, R, true>(s.pm, N, tc, q, x64);
+#pragma unroll
+        for (int k = 0; k < R; ++k) rh[k] = has(k) ? s.t1[tc * NX + row(k)] + a[k] + h.v[k] : 0.0;
+        eta64 = block_sum2(eta_of(rh, zh), red, par);
+        exact = !(eta64 > c_eps);
+      }
+      if (exact) {
+        flush();
+        exact_rhat_rows<NX, R, true>(s, lam, tc, q, ok, N);
+#pragma unroll
+        for (int k = 0; k < R; ++k) rh[k] = has(k) ? s.t1[tc * NX + row(k)] : 0.0;
+        eta64 = block_sum2(eta_of(rh, zh), red, par);
+      }
+      if (!(fabs(eta64) > c_eps && it <= c_maxit - 1) || !(eta64 == eta64)) {
+        if (!exact) flush();
+        nrep_out = nupd;
+        break;
+      }
+      const double etas = eta64 * s2;
+      if (bad || nupd >= c_maxref || it >= it_cap || !(etas > 0.0) ||
+          (progressed && !at_check && eta64 > (cut ? c_upd : kUpdateStagnation) * prev64)) {
+        if (!exact) flush();
+        par_io = par;
+        return fp64_finish(s, lam, it, c_maxit, c_eps, red, par_io, nupd);
+      }
+      it_stop = next_stop(it, it - (int)cst[11], it_cap);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        cst[4] = eta64;
+        cst[5] = etas;
+        cst[9] = (double)nupd;
+        cst[11] = (double)it;
+      }
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        r[k] = has(k) ? (float)(scale * rh[k]) : 0.f;
+        z[k] = has(k) ? (float)(scale * zh[k]) : 0.f;
+      }
+      if (etas > kRestartRatio * eta) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) p[k] = 0.f;
+      }
+      etap = etas;
+      trig = (float)fmax(check_at, c_upd * etas);
+      hi = (float)(kDivergeRatio * etas);
+    }
+    const float beta = quot32(etap, eta);
+#pragma unroll
+    for (int k = 0; k < R; ++k) p[k] = fmaf(beta, p[k], z[k]);
+    eta = etap;
+  }
+  par_io = par;
+  return PcgOut{it, eta64, nrep_out};
+}
+
 
 // ---------------------------------------------------------------- recovery (pcg.py:290-348)
 // x_t = -Qi_t (q_t + An_{t-1}^T lam_t + A_t^T lam_{t+1}), An_{-1} = I, An = -I;
@@ -1579,9 +1919,7 @@ __device__ inline SmemView carve_smem(unsigned char* sm, int nx, int K, int prec
   v.dvals = v.red + 128;
   unsigned char* p = sm + 136 * sizeof(double);
   v.vec = p;
-  size_t vb = (precision == DMPC_PREC_FP64) ? 5 * (size_t)K * nx * sizeof(double)
-                                            : align_up(5 * (size_t)(K + 2) * pad_ld(nx) * sizeof(float), 16);
-  v.blocks = reinterpret_cast<float*>(p + vb);
+  v.blocks = reinterpret_cast<float*>(p + pcg_vec_bytes(nx, K, precision, DMPC_CFG));
   return v;
 }
 
@@ -1601,6 +1939,26 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
   }
   float* v = reinterpret_cast<float*>(sv.vec);
   if (sh_scaled_bad) return fp64_finish(s, lam, 0, P.pcg_max_iter, P.pcg_tol_epsilon, sv.red, par, 0);
+#if DMPC_CFG == 2
+  // two CTAs per SM: the row PCG with one register copy of each W block
+  if (s.K * rows_tpk(s.nx) <= (int)blockDim.x) {
+    switch (s.nx) {
+#define DMPC_ROWS_T(NXV)                                                                                   \
+  case NXV:                                                                                                \
+    return pcg_rows_t<NXV, rows_tpk(NXV)>(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement, \
+                                          P.inner_rel_tol, sv.red, par);
+      DMPC_ROWS_T(3)
+      DMPC_ROWS_T(4)
+      DMPC_ROWS_T(6)
+      DMPC_ROWS_T(7)
+      DMPC_ROWS_T(8)
+      DMPC_ROWS_T(12)
+      DMPC_ROWS_T(13)
+#undef DMPC_ROWS_T
+      default: break;
+    }
+  }
+#else
   if (s.K * ((s.nx + 3) / 4) <= (int)blockDim.x) {
     switch (s.nx) {
 #define DMPC_ROWS(NXV)                                                                                   \
@@ -1618,6 +1976,7 @@ __device__ PcgOut solve_qp(const Inst& s, const dmpc_solver_params& P, SmemView&
       default: break;
     }
   }
+#endif
   return pcg_mixed_scaled(s, lam, v, P.pcg_max_iter, P.pcg_tol_epsilon, P.max_refinement, P.inner_rel_tol,
                           sv.red, par);
 }

@@ -83,7 +83,7 @@ def test_linesearch_mixed_matches_oracle():
 @pytest.mark.parametrize("nx", [5, 6])
 def test_ill_conditioned_qps_hand_over_to_fp64_and_match_oracle(nx):
     """State weights over 1e-6..1e6 (cond(S) 1e7..1e9): the FP32 recursion stalls on most of these
-    QPs.  The stall detection (a segment cut after max(4 x the previous one, 200) iterations, then
+    QPs.  The stall detection (a segment cut after max(2 x the previous one, 200) iterations, then
     the stagnation rule) hands them to the FP64 recurrence after a few hundred FP32 iterations;
     without it a stalled QP runs half the 10000-iteration budget in FP32 before the FP64 finish, so
     a count below 5000 shows the hand-over.  nx=6 takes the compile-time row PCG, nx=5 the generic
