@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
     ap.add_argument("--cta-config", default="auto", choices=["auto", "wide", "rows", "dual"],
                     help="CTA shape of the solver kernels (dmpc_solver_params.cta_config)")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="dmpc_solver_params.threads_per_block (0: automatic)")
     ap.add_argument("--blocks-in-smem", type=int, default=-1, choices=[-1, 0, 1],
                     help="dmpc_solver_params.blocks_in_smem (-1: shared memory when they fit)")
     ap.add_argument("--workload", default="quadrotor", choices=["quadrotor", "attitude", "mixed", "stress", "rollout", "rollout_spacecraft"],
@@ -153,14 +155,20 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ workload
+def launch_shape(sp, args):
+    """The launch-shape overrides of the command line (automatic by default)."""
+    sp["cta_config"] = CTA_CONFIGS[args.cta_config]
+    sp["threads_per_block"] = args.threads
+    sp["blocks_in_smem"] = args.blocks_in_smem
+
+
 def build(args, rank):
     from diffmpc_b200 import workloads
 
     dyn, st, bt, sp = workloads.quadrotor(B=args.batch, N=args.horizon, seed=1002 + rank)
     sp["precision"] = args.precision
     sp["pcg"]["tol_epsilon"] = args.pcg_tol
-    sp["cta_config"] = CTA_CONFIGS[args.cta_config]
-    sp["blocks_in_smem"] = args.blocks_in_smem
+    launch_shape(sp, args)
     return dyn, st, bt, sp
 
 
@@ -657,6 +665,7 @@ def run_other_workload(args):
     if args.workload == "attitude":
         B = args.batch if args.batch != 4096 else 1024
         dyn, st, bt, sp = workloads.attitude(B=B)
+        launch_shape(sp, args)
         res = {}
         for prec in ("mixed", "fp64"):
             sp2 = dict(sp, precision=prec)
@@ -818,9 +827,19 @@ def run_other_workload(args):
                 return sol, w
 
             ms, (sol, w) = _timed(step, args.steps, args.warmup)
+            # QP solves whose FP64 recurrence ran out of pcg.max_iter before the stopping test held
+            its64 = solver.last_forward_pcg_record[1].cpu() if prec == "mixed" else sol.num_pcg_iters.cpu()
+            at_budget = (its64 >= sp["pcg"]["max_iter"]).any(dim=1)
             out[prec] = (ms, sol.controls.detach().cpu(), w["weights_penalization_reference_state_trajectory"].grad.cpu(),
-                         sol.num_pcg_iters.sum(dim=1).double().mean().item(), precision_record(solver, sol))
+                         sol.num_pcg_iters.sum(dim=1).double().mean().item(), precision_record(solver, sol), at_budget)
         c64, g64 = out["fp64"][1], out["fp64"][2]
+        rel_c = _rel_per_instance(out["mixed"][1], c64)
+        outl = [int(i) for i in torch.nonzero(rel_c > 1e-6).flatten()]
+        line.update(qp_budget_exhausted={"mixed_instances": int(out["mixed"][5].sum()),
+                                         "fp64_instances": int(out["fp64"][5].sum()),
+                                         "control_outliers_with_a_qp_at_budget": sum(
+                                             1 for i in outl if bool(out["mixed"][5][i] or out["fp64"][5][i])),
+                                         "control_outliers": len(outl)})
         line.update(metric="fwd+bwd MPC solves/s, linear nx=24 nu=8 N=128, diag Q 1e-3..1e3, B=%d" % B,
                     value=B / (out["mixed"][0] * 1e-3), fp64_value=B / (out["fp64"][0] * 1e-3),
                     max_rel_control_diff_mixed_vs_fp64=float((out["mixed"][1] - c64).abs().max() / c64.abs().max()),

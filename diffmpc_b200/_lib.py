@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libdmpc.so")
 
 ABI_VERSION = 3
 DMPC_OK = 0
+DMPC_ERR_INVALID = 1
 DMPC_ERR_CUDA = 3
 DMPC_MAX_NX = 32
 DMPC_MAX_NU = 16
@@ -44,6 +45,7 @@ EXPORTED_SYMBOLS = (
     "dmpc_solve_fwd_noalloc",
     "dmpc_rollout_fwd",
     "dmpc_rollout_adj",
+    "dmpc_psd_project",
 )
 
 _p = ctypes.c_void_p
@@ -233,6 +235,8 @@ def load():
         ctypes.POINTER(Group), ctypes.POINTER(Rollout), ctypes.POINTER(Adjoint), ctypes.POINTER(RolloutAdjoint),
         ctypes.POINTER(SolverParams), _p, ctypes.c_size_t, _p,
     ]
+    lib.dmpc_psd_project.restype = ctypes.c_int
+    lib.dmpc_psd_project.argtypes = [ctypes.c_int, ctypes.c_int, _p, _f64, _p, _p]
     if lib.dmpc_abi_version() != ABI_VERSION:
         raise DmpcError("libdmpc.so ABI version mismatch")
     _lib = lib

@@ -49,6 +49,31 @@ __device__ __forceinline__ double block_sum_f32w(float v, double* red, int& pari
   return s;
 }
 
+// block_sum_f32w with a broadcast second stage: every thread reads all warp sums (FP64, two per
+// 16-byte load) and adds them in one fixed order, instead of a butterfly of FP64 shuffles.  The
+// CTA must have an even number of warps, at most 16.
+__device__ __forceinline__ double block_sum_f32b(float v, double* red, int& parity) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(DMPC_FULL_MASK, v, o);
+  double* buf = red + (parity << 6);
+  if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = (double)v;
+  __syncthreads();
+  const double2* b2 = reinterpret_cast<const double2*>(buf);
+  const int np = (int)(blockDim.x >> 6);
+  double s = 0.0;
+  if (np == 4) {
+    const double2 a = b2[0], b = b2[1], c = b2[2], d = b2[3];
+    s = ((a.x + a.y) + (b.x + b.y)) + ((c.x + c.y) + (d.x + d.y));
+  } else {
+    for (int i = 0; i < np; ++i) {
+      const double2 a = b2[i];
+      s += a.x + a.y;
+    }
+  }
+  parity ^= 1;
+  return s;
+}
+
 // Smallest power of two >= the CTA's warp count (the width of block_sum_f32w's second stage).
 __device__ __forceinline__ int warp_pow2() {
   const int nw = blockDim.x >> 5;

@@ -340,6 +340,111 @@ __global__ void __launch_bounds__(256) k_pcg_dense(int N, int nx, int nu, const 
   }
 }
 
+// ---------------------------------------------------------------- PSD projection (jax_utils.py:75-95)
+// project_matrix_onto_positive_semidefinite_cone for a batch of n x n matrices, n <= 32: one warp
+// per matrix.  As jnp.linalg.eigh does by default, the input is symmetrized, (M + M^T) / 2; its
+// eigen-decomposition comes from the cyclic Jacobi method (Golub and Van Loan, Matrix
+// Computations, sections 8.5.2-8.5.3: for each off-diagonal (p, q) the rotation with
+// tau = (a_qq - a_pp) / (2 a_pq), t = sign(tau) / (|tau| + sqrt(1 + tau^2)), c = 1 / sqrt(1 + t^2),
+// s = t c zeroes a_pq), sweeping until the off-diagonal mass is below (eps_64 ||A||_F)^2 or after
+// kPsdMaxSweeps sweeps.  Lane k owns row k of the two rotated columns of A and V.  The result is
+// V diag(max(lambda, minimum_eigenvalue)) V^T, symmetrized as the reference does; the projection
+// onto the cone does not depend on the order or signs of the eigenvectors.  A matrix with a NaN or
+// infinite entry gives all-NaN output (its eigen-decomposition is not a number, and jnp.maximum
+// propagates NaN).  Shared memory per warp: A, V (n x n) and the clipped eigenvalues (n).
+constexpr int kPsdMaxSweeps = 50;
+constexpr int kPsdWarps = 4;
+__global__ void __launch_bounds__(32 * kPsdWarps) k_psd_project(int batch, int n, const double* in,
+                                                                  double min_eig, double* out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long b = (long long)blockIdx.x * kPsdWarps + warp;
+  if (b >= batch) return;  // the whole warp leaves; the kernel has no CTA barrier
+  const int nn = n * n;
+  double* A = reinterpret_cast<double*>(smem) + (size_t)warp * (2 * nn + n);
+  double* V = A + nn;
+  double* mu = V + nn;
+  const double* M = in + (size_t)b * nn;
+  double fro = 0.0;
+  for (int i = lane; i < nn; i += 32) {
+    const int r = i / n, c = i - r * n;
+    const double a = 0.5 * (M[i] + M[c * n + r]);
+    A[i] = a;
+    V[i] = (r == c) ? 1.0 : 0.0;
+    fro += a * a;
+  }
+  fro = warp_sum(fro);
+  double* o = out + (size_t)b * nn;
+  if (!(fro <= 1.7976931348623157e308)) {  // a NaN or infinite entry: the eigen-decomposition is NaN
+    for (int i = lane; i < nn; i += 32) o[i] = __longlong_as_double(0x7ff8000000000000ll);
+    return;
+  }
+  __syncwarp();
+  const double tol = 4.930380657631324e-32 * fro;  // (2^-52)^2 ||A||_F^2
+  for (int sweep = 0; sweep < kPsdMaxSweeps; ++sweep) {
+    double off = 0.0;
+    for (int i = lane; i < nn; i += 32) {
+      const int r = i / n;
+      if (r != i - r * n) off += A[i] * A[i];
+    }
+    off = warp_sum(off);
+    if (!(off > tol)) break;  // converged, or not a number
+    for (int p = 0; p < n - 1; ++p) {
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = A[p * n + q];
+        if (apq == 0.0) continue;  // the same shared value in every lane
+        const double app = A[p * n + p], aqq = A[q * n + q];
+        const double tau = (aqq - app) / (2.0 * apq);
+        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        const double c = 1.0 / sqrt(1.0 + t * t), sn = t * c;
+        double akp = 0.0, akq = 0.0, vkp = 0.0, vkq = 0.0;
+        if (lane < n) {
+          akp = A[lane * n + p];
+          akq = A[lane * n + q];
+          vkp = V[lane * n + p];
+          vkq = V[lane * n + q];
+        }
+        __syncwarp();
+        if (lane < n) {
+          if (lane != p && lane != q) {
+            const double nkp = c * akp - sn * akq, nkq = sn * akp + c * akq;
+            A[lane * n + p] = nkp;
+            A[p * n + lane] = nkp;
+            A[lane * n + q] = nkq;
+            A[q * n + lane] = nkq;
+          }
+          V[lane * n + p] = c * vkp - sn * vkq;
+          V[lane * n + q] = sn * vkp + c * vkq;
+        }
+        if (lane == 0) {
+          A[p * n + p] = app - t * apq;
+          A[q * n + q] = aqq + t * apq;
+          A[p * n + q] = 0.0;
+          A[q * n + p] = 0.0;
+        }
+        __syncwarp();
+      }
+    }
+  }
+  if (lane < n) {
+    const double l = A[lane * n + lane];
+    mu[lane] = (l < min_eig) ? min_eig : l;
+  }
+  __syncwarp();
+  // P = V diag(mu) V^T into A, then out = (P + P^T) / 2
+  for (int i = lane; i < nn; i += 32) {
+    const int r = i / n, c = i - r * n;
+    double a = 0.0;
+    for (int k = 0; k < n; ++k) a = fma(V[r * n + k] * mu[k], V[c * n + k], a);
+    A[i] = a;
+  }
+  __syncwarp();
+  for (int i = lane; i < nn; i += 32) {
+    const int r = i / n, c = i - r * n;
+    o[i] = 0.5 * (A[i] + A[c * n + r]);
+  }
+}
+
 // ---------------------------------------------------------------- FP32 FMA throughput probe
 // Eight independent FMA chains per thread; used only to measure the FP32 CUDA-core
 // peak that serves as the roofline denominator of the (shared-memory resident) PCG.
@@ -822,6 +927,20 @@ int dmpc_kkt_recover(int batch, int N, int nx, int nu, const double* lambda, con
   if (e != cudaSuccess) return cuda_rc(e);
   k_recover_dense<<<batch, 256, sm, reinterpret_cast<cudaStream_t>(stream)>>>(N, nx, nu, lambda, As_next, As, Bs,
                                                                               Qinv, qvec, Rinv, rvec, states, controls);
+  return cuda_rc(cudaGetLastError());
+}
+
+int dmpc_psd_project(int batch, int n, const double* matrices, double minimum_eigenvalue, double* out,
+                     void* stream) {
+  if (batch < 0 || n < 1 || n > 32 || (batch > 0 && (!matrices || !out))) return DMPC_ERR_INVALID;
+  if (batch == 0) return DMPC_OK;
+  const size_t sm = (size_t)kPsdWarps * (2 * (size_t)n * n + n) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_psd_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return cuda_rc(e);
+  const long long blocks = ((long long)batch + kPsdWarps - 1) / kPsdWarps;
+  if (blocks > 0x7fffffffLL) return DMPC_ERR_INVALID;
+  k_psd_project<<<(unsigned)blocks, 32 * kPsdWarps, sm, reinterpret_cast<cudaStream_t>(stream)>>>(
+      batch, n, matrices, minimum_eigenvalue, out);
   return cuda_rc(cudaGetLastError());
 }
 

@@ -1479,14 +1479,14 @@ __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec
     f[2] = ok ? a[2] + b[2] + u.z : 0.f;
     f[3] = ok ? a[3] + b[3] + u.w : 0.f;
   };
+  // rows past NX and idle threads hold exact zeros in every FP32 vector (set so at the start and
+  // kept by the recurrences, whose operator terms vanish there), so a dot product needs no mask
   auto dot32 = [&](const float* a, const float* b) {
     float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < R; ++k)
-      if (has(k)) acc = fmaf(a[k], b[k], acc);
+    for (int k = 0; k < R; ++k) acc = fmaf(a[k], b[k], acc);
     return acc;
   };
-  const int w2 = warp_pow2();
   // FP64 exchange vector (knots -1..K) after the four FP32 vectors, then the solve's constants
   auto x64_of = [&]() { return reinterpret_cast<double*>(as_shared(vec + 4 * span)) + NX; };
   {
@@ -1606,7 +1606,7 @@ __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec
         pull(w, pv, upp, f);
 #pragma unroll
         for (int k = 0; k < R; ++k) u[k] = -(p[k] + f[k]);
-        vden = block_sum_f32w(dot32(p, u), red, par, w2);
+        vden = block_sum_f32b(dot32(p, u), red, par);
         const float alpha = quot32(eta, vden);
 #pragma unroll
         for (int k = 0; k < R; ++k) {
@@ -1619,7 +1619,7 @@ __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec
         pull(w, rv, upr, f);
 #pragma unroll
         for (int k = 0; k < R; ++k) z[k] = r[k] - f[k];
-        etap = block_sum_f32w(dot32(r, z), red, par, w2);
+        etap = block_sum_f32b(dot32(r, z), red, par);
         ++it;
         const float etaf = (float)etap;
         if (!(etaf > trig) || etaf > hi || it >= it_stop || !(vden == vden)) break;

@@ -308,6 +308,16 @@ int dmpc_schur_assemble(int batch, int N, int nx, int nu, const double* As_next,
                         double* gamma, void* workspace, size_t workspace_bytes, void* stream);
 size_t dmpc_schur_workspace_size(int batch, int N, int nx);
 
+/* project_matrix_onto_positive_semidefinite_cone (jax_utils.py:75-95), as SQPSolver.get_cost_terms
+ * applies it to every cost Hessian with minimum_eigenvalue 1e-9 (sqp.py:191-196): for each of the
+ * `batch` row-major n x n matrices (1 <= n <= 32) in device memory, out = V diag(max(lambda,
+ * minimum_eigenvalue)) V^T of the symmetrized input (M + M^T) / 2 (jnp.linalg.eigh symmetrizes by
+ * default), itself symmetrized.  FP64 Jacobi eigen-decomposition, one warp per matrix.  `out` may
+ * equal `matrices`.  A matrix with a NaN or infinite entry gives all-NaN output.  The fused solver does not call it: its cost Hessians are diagonal, where the
+ * projection is max(h_ii, 1e-9) exactly. */
+int dmpc_psd_project(int batch, int n, const double* matrices, double minimum_eigenvalue, double* out,
+                     void* stream);
+
 /* solve_KKT_Schur on the dense S / Phiinv layout (pcg.py:350-445), FP64, with the
  * reference's stopping rule; then (x, u) from lambda (pcg.py:290-348).
  * lambda_guess (batch,K,nx) -> lambda, states (batch,K,nx), controls (batch,K,nu),

@@ -62,8 +62,10 @@ class SQPSolution(NamedTuple):  # sqp.py:38-57
 
 
 def project_psd(M, minimum_eigenvalue):
-    """PSD projection by eigen-decomposition (jax_utils.py:75-95)."""
-    S, V = torch.linalg.eigh(M)
+    """PSD projection by eigen-decomposition (jax_utils.py:75-95).  The input is symmetrized first,
+    (M + M^T) / 2, as jnp.linalg.eigh does by default (symmetrize_input=True); torch's eigh would
+    otherwise read only the lower triangle."""
+    S, V = torch.linalg.eigh(0.5 * (M + M.mT))
     S = torch.clamp(S, min=minimum_eigenvalue)
     proj = V @ (torch.diag_embed(S) @ V.mT)
     return 0.5 * (proj + proj.mT)
