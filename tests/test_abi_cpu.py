@@ -146,3 +146,26 @@ def test_jax_shim_is_import_guarded():
     if jax_shim.jax is None:
         with pytest.raises(ImportError):
             jax_shim.make_jax_solve(None, {})
+
+
+def test_automatic_launch_shape_puts_two_headline_instances_on_an_sm():
+    """Mixed precision, quadrotor N=60 (K ceil(13/4) = 244 > 128 threads of the one-CTA row
+    layout), more instances than SMs: the automatic choice is the two-CTA configuration, whose
+    workspace holds two slots per SM (148 SMs assumed without a device), twice the one-CTA row
+    configuration's.  FP64 precision keeps one CTA per SM, and a batch of at most one instance per
+    SM takes one slot per instance."""
+    lib = _lib.load()
+    p = _lib.SolverParams()
+    lib.dmpc_default_params(p)
+    assert p.precision == _lib.PREC_MIXED and p.cta_config == _lib.CTA_AUTO
+    g = _group(N=60, batch=4096)
+    auto = lib.dmpc_workspace_size(1, g, p)
+    p.cta_config = _lib.CTA_ROWS
+    rows = lib.dmpc_workspace_size(1, g, p)
+    p.cta_config = _lib.CTA_DUAL
+    dual = lib.dmpc_workspace_size(1, g, p)
+    assert auto == dual and (auto - 256) == 2 * (rows - 256)
+    p.cta_config = _lib.CTA_AUTO
+    assert lib.dmpc_workspace_size(1, _group(N=60, batch=100), p) - 256 == 100 * (rows - 256) // 148
+    p.precision = _lib.PREC_FP64
+    assert lib.dmpc_workspace_size(1, g, p) == rows
