@@ -20,6 +20,7 @@ installed offline) on the host cores, one instance per step.
 """
 
 import argparse
+import copy
 import json
 import math
 import os
@@ -57,6 +58,7 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--fp64-sample", type=int, default=8, help="instances timed one-per-launch in FP64")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / fp64 / e2e legs")
+    ap.add_argument("--no-other", action="store_true", help="skip the other workload shapes in the headline run")
     ap.add_argument("--cta-config", default="auto", choices=["auto", "wide", "rows", "dual"],
                     help="CTA shape of the solver kernels (dmpc_solver_params.cta_config)")
     ap.add_argument("--threads", type=int, default=0,
@@ -589,6 +591,9 @@ def run_ours(args):
         # ---- CPU baseline: float64 oracle on the host cores, with the oracle check
         if pool is not None:
             line["cpu_baseline"] = cpu_baseline(args, sol, grads, bt, dyn, st, sp, pool, workers)
+        # ---- the other workload shapes, one GPU
+        if world == 1 and not args.no_other:
+            line["other_workloads"] = other_workloads(args)
     if pool is not None:
         pool.close()
         pool.join()
@@ -848,7 +853,35 @@ def run_other_workload(args):
                     grads_mixed_vs_fp64=_dist(_rel_per_instance(out["mixed"][2], g64), 1e-5),
                     pcg_iters_mixed=out["mixed"][3], pcg_iters_fp64=out["fp64"][3],
                     refinement_steps=out["mixed"][4]["replacements_per_qp"], precision_record=out["mixed"][4])
-    print(json.dumps(line), flush=True)
+    return line
+
+
+# The other workload shapes measured inside the default run (one GPU, after the headline), so that
+# the line the default run prints carries them too: (workload, batch or None for its default,
+# steps, warm-up steps).  The precision-stress shape runs on a 1024-instance slice of its
+# 16384-instance batch to keep the run within minutes (`--workload stress` runs all of it).
+OTHER_WORKLOADS = (("attitude", None, 3, 3), ("rollout", None, 3, 3), ("rollout_spacecraft", None, 3, 3),
+                   ("mixed", None, 2, 1), ("stress", 1024, 1, 1))
+
+
+def other_workloads(args):
+    out = {}
+    for name, batch, steps, warmup in OTHER_WORKLOADS:
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup = name, steps, warmup
+        a.batch = batch if batch is not None else 4096  # 4096: the workload's own default batch
+        a.cta_config, a.threads, a.blocks_in_smem = "auto", 0, -1
+        t0 = time.perf_counter()
+        try:
+            line = run_other_workload(a)
+        except Exception as e:  # noqa: BLE001 - the headline line must still print
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+            continue
+        line["wall_s"] = time.perf_counter() - t0
+        for k in ("impl", "unit", "n_gpus", "data", "workload"):
+            line.pop(k, None)
+        out[name] = line
+    return out
 
 
 def main():
@@ -856,7 +889,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
     elif args.workload != "quadrotor":
-        run_other_workload(args)
+        print(json.dumps(run_other_workload(args)), flush=True)
     else:
         run_ours(args)
 

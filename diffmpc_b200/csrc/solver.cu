@@ -621,8 +621,8 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
   // configuration, unless the caller chose one:
   // - two CTAs per SM (pcg_rows_t) when every group is mixed precision with a compile-time row
   //   layout whose K rows_tpk(nx) threads fit 256, the one-CTA row layout would need more than
-  //   128 threads (so that it would hold one instance per SM), and the batch has more instances
-  //   than SMs (measured: quadrotor N=60, B=4096, 22 % faster than the one-CTA row layout);
+  //   three warps, and the batch has more instances than SMs (measured: quadrotor N=60, B=4096,
+  //   22 % faster than the one-CTA row layout; attitude N=50, B=1024, 102 threads, 4 %);
   // - else the row configuration when every group has a compile-time row PCG whose K ceil(nx/4)
   //   threads fit 384, or is ragged (instances too long for it take the generic PCG inside the
   //   same launch);
@@ -635,7 +635,7 @@ int fill_args(int n_groups, const dmpc_group* groups, const dmpc_adjoint* adj, c
     for (int k = 0; k < n_groups; ++k) {
       const int nx = groups[k].nx, K = groups[k].horizon + 1;
       rows = rows && (rows_path(p, nx, K, 384) || (p->precision == DMPC_PREC_MIXED && rows_nx(nx) && groups[k].horizons));
-      dual = dual && rows_path(p, nx, K, 256, kCfgDual) && K * ((nx + 3) / 4) > 128;
+      dual = dual && rows_path(p, nx, K, 256, kCfgDual) && K * ((nx + 3) / 4) > 96;
     }
     if (dual && total > dev.sms) cfg = kCfgDual;
     else if (rows) cfg = kCfgRows;

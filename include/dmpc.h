@@ -118,14 +118,18 @@ typedef struct dmpc_solver_params {
   int32_t cta_config;             /* DMPC_CTA_*: CTA shape of the solver kernels (diffmpc_b200.autotune) */
 } dmpc_solver_params;
 
-/* dmpc_solver_params.cta_config.  AUTO: ROWS when every group is mixed precision with a
- * compile-time row PCG (nx in {3,4,6,7,8,12,13}) whose K ceil(nx/4) threads fit 384 (or is ragged:
- * its longer instances take the generic PCG), else WIDE. */
+/* dmpc_solver_params.cta_config.  AUTO: DUAL when every group is mixed precision with a
+ * compile-time row layout (nx in {3,4,6,7,8,12,13}) whose K rows_tpk(nx) threads fit 256
+ * (rows_tpk = 1, 2, 4 for nx <= 4, 8, 16), its one-CTA row layout would need more than three warps
+ * and the batch has more instances than SMs; else ROWS when every group has a row layout whose
+ * K ceil(nx/4) threads fit 384 (or is ragged: its longer instances take the generic PCG); else
+ * WIDE. */
 #define DMPC_CTA_AUTO 0
 #define DMPC_CTA_WIDE 1 /* up to 512 threads (threads_per_block or automatic), one CTA per SM */
 #define DMPC_CTA_ROWS 2 /* 256..384 threads (threads_per_block or automatic), one CTA per SM; up to 255
                            registers per thread at 256 threads, 168 above, for the row PCG */
-#define DMPC_CTA_DUAL 3 /* 256 threads, two CTAs per SM */
+#define DMPC_CTA_DUAL 3 /* 256 threads, two CTAs per SM, 128 registers per thread; mixed precision
+                           takes the row PCG with one register copy of each scaled block */
 
 /* One group = instances sharing model, nx, nu and max horizon (a batch).
  * Per-instance horizons may differ (ragged batch): arrays are padded to K = horizon + 1
