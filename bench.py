@@ -53,6 +53,7 @@ def parse_args():
     ap.add_argument("--horizon", type=int, default=60)
     ap.add_argument("--pcg-tol", type=float, default=1e-20)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--pcg-max-iter", type=int, default=0, help="pcg.max_iter (0: the workload's own)")
     ap.add_argument("--cpu-sample", type=int, default=16, help="instances per CPU-baseline run (and pool size cap)")
     ap.add_argument("--cpu-runs", type=int, default=3, help="CPU-baseline runs (median reported)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
@@ -817,6 +818,8 @@ def run_other_workload(args):
         B = args.batch if args.batch != 4096 else 16384
         dyn, st, bt, sp = workloads.linear_stress(B=B)
         sp["pcg"]["tol_epsilon"] = args.pcg_tol
+        if args.pcg_max_iter > 0:
+            sp["pcg"]["max_iter"] = args.pcg_max_iter
         sp["num_scp_iteration_max"] = 2
         out = {}
         for prec in ("mixed", "fp64"):
@@ -846,6 +849,7 @@ def run_other_workload(args):
                                              1 for i in outl if bool(out["mixed"][5][i] or out["fp64"][5][i])),
                                          "control_outliers": len(outl)})
         line.update(metric="fwd+bwd MPC solves/s, linear nx=24 nu=8 N=128, diag Q 1e-3..1e3, B=%d" % B,
+                    pcg_max_iter=sp["pcg"]["max_iter"],
                     value=B / (out["mixed"][0] * 1e-3), fp64_value=B / (out["fp64"][0] * 1e-3),
                     max_rel_control_diff_mixed_vs_fp64=float((out["mixed"][1] - c64).abs().max() / c64.abs().max()),
                     max_rel_grad_diff_mixed_vs_fp64=float((out["mixed"][2] - g64).abs().max() / g64.abs().max()),
