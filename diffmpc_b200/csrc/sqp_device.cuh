@@ -1397,9 +1397,10 @@ __device__ __noinline__ PcgOut pcg_rows_scaled(const Inst& s, double* lam, float
 // So that the reduce-scatter needs no selects, lane q keeps its W columns in an order that puts
 // the columns it sends in the first half of its registers at each round: register group g holds
 // column group g ^ (TPK - 1 - q).  The lower product reads v_{t-1} in that order (float4 loads).
-// Threads past the last knot idle on knot 0 with zero coefficients, store nothing and add zeros
-// to the reductions.  Everything else (scaling, FP64 residual replacement, stall detection,
-// hand-over to the FP64 recurrence, stopping test) follows pcg_rows_scaled line by line.
+// Threads past the last knot idle on knot 0 (their F^ v reads knot K, zero) with zero
+// coefficients, store nothing and add zeros to the reductions.  Everything else (scaling, FP64
+// residual replacement, stall detection, hand-over to the FP64 recurrence, stopping test) follows
+// pcg_rows_scaled line by line.
 template <int NX, int TPK>
 __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec, int max_iter, double eps,
                                           int max_ref, double upd_rel, double* red, int& par_io) {
@@ -1421,6 +1422,9 @@ __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec
   const bool ok = (int)threadIdx.x < TPK * K;
   const int q = ok ? lane_q : 0;
   const int tc = ok ? (int)threadIdx.x / TPK : 0;
+  // the knot an idle thread's F^ reads: K, whose upper-term segment is never written (zero), and
+  // whose lower term meets the thread's zero coefficients, so its F^ v is zero without a select
+  const int tp = ok ? tc : K;
   auto row = [&](int k) { return R * q + k; };
   auto has = [&](int k) { return ok && R * q + k < NX; };
   auto cgrp = [&](int g) { return g ^ (TPK - 1 - lane_q); };  // column group of register group g
@@ -1461,7 +1465,7 @@ __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec
       a[k] = 0.f;
       b[k] = 0.f;
     }
-    const float* vm = v + (tc - 1) * PD;
+    const float* vm = v + (tp - 1) * PD;
 #pragma unroll
     for (int g = 0; g < TPK; ++g) {
       const float4 y = *reinterpret_cast<const float4*>(vm + 4 * cgrp(g));
@@ -1473,11 +1477,11 @@ __device__ __noinline__ PcgOut pcg_rows_t(const Inst& s, double* lam, float* vec
         b[k] = fmaf(w[k][4 * g + 3], y.w, b[k]);
       }
     }
-    const float4 u = *reinterpret_cast<const float4*>(up + tc * PD + R * q);
-    f[0] = ok ? a[0] + b[0] + u.x : 0.f;
-    f[1] = ok ? a[1] + b[1] + u.y : 0.f;
-    f[2] = ok ? a[2] + b[2] + u.z : 0.f;
-    f[3] = ok ? a[3] + b[3] + u.w : 0.f;
+    const float4 u = *reinterpret_cast<const float4*>(up + tp * PD + R * q);
+    f[0] = a[0] + b[0] + u.x;
+    f[1] = a[1] + b[1] + u.y;
+    f[2] = a[2] + b[2] + u.z;
+    f[3] = a[3] + b[3] + u.w;
   };
   // rows past NX and idle threads hold exact zeros in every FP32 vector (set so at the start and
   // kept by the recurrences, whose operator terms vanish there), so a dot product needs no mask
