@@ -105,3 +105,20 @@ def test_dual_and_row_configurations_agree_on_a_headline_batch():
         err = ((c - ref).abs().amax(dim=(1, 2)) / ref.abs().amax(dim=(1, 2))).max()
         assert float(err) < 1e-6, (cfg, float(err))
         assert torch.equal(sol.status.cpu(), s64.status.cpu())
+
+
+def test_dual_solves_are_deterministic():
+    """Fixed-order reductions and shuffles: two solves of the same batch (forward and adjoint)
+    give bit-equal controls, duals, iteration counts and gradients."""
+    dyn, st, bt, sp = workloads.quadrotor(B=300, N=60, seed=1002)  # more instances than SMs: AUTO takes DUAL
+    sp["precision"] = "mixed"
+    sp["pcg"]["tol_epsilon"] = 1e-20
+    sp["num_scp_iteration_max"] = 3
+    outs = []
+    for _ in range(2):
+        w = {"initial_state": bt["initial_state"].clone().to(DEV).requires_grad_(True)}
+        _, sol = gpu_solve(dyn, st, bt, sp, weights=w)
+        (sol.controls[:, 0] ** 2).sum().backward()
+        outs.append((sol.controls.detach().cpu(), sol.dual.detach().cpu(), sol.num_pcg_iters.cpu(), w["initial_state"].grad.cpu()))
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
