@@ -242,3 +242,30 @@ def test_rl_quadrotor_notebook_rollout_on_gpu():
     loss = -float(roll(torch.tensor(x0, device=DEV), bp, {}, initial_guess=g).sum())
     want = -241.93737859418738
     assert abs(loss - want) < 2e-3 * abs(want), loss
+
+
+def test_rollout_in_the_two_cta_configuration_matches_oracle():
+    """The fused rollout's forward and reverse sweeps in the two-CTA configuration (the row PCG
+    with one register copy of each scaled block, nx=8: two threads per knot), against the oracle's
+    rollout at the mixed-precision bars."""
+    dyn, st, bt, sp, (A, Bm, b), _, p = _setup("mixed", True)
+    sp["cta_config"] = 3  # DMPC_CTA_DUAL
+    solver = SQPSolver(OptimalControlProblem(dyn, st), params=sp)
+    T = 3
+    w = {k: p[k].clone().requires_grad_(True) for k in (KW, KU)}
+    roll = ClosedLoopRollout(solver, A.to(DEV), Bm.to(DEV), b.to(DEV), T, warm_start=True)
+    cost = roll(p["initial_state"], p, w)
+    cost.sum().backward()
+    torch.cuda.synchronize()
+    osolver = oracle_solver(dyn, st, sp)
+    op = tensor_params(bt)
+    ow = {k: op[k].clone().requires_grad_(True) for k in (KW, KU)}
+    B = op["initial_state"].shape[0]
+    ocost, ous, _ = oracle_rollout(osolver, op, op["initial_state"], ow, A.expand(B, 8, 8), Bm.expand(B, 8, 4),
+                                   b.expand(B, 8), T, warm_start=True)
+    ocost.sum().backward()
+    assert rel_err(cost, ocost) < 1e-6
+    for k in range(T):
+        assert rel_err(roll.last.controls[k][:, 0], ous[k]) < 1e-6, k
+    for k in (KW, KU):
+        assert rel_err(w[k].grad, ow[k].grad) < 1e-5, k
